@@ -1,0 +1,180 @@
+"""ctypes binding of ``libcib200.so`` (the C ABI declared in ``include/cib200.h``).
+
+The library is built in-tree by :mod:`concrete_impact_b200.build`.  Loading it needs no
+GPU; every compute entry point does, and :func:`require_cuda` makes that failure loud:
+there is no CPU fallback anywhere in this package.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "libcib200.so"
+CIB_NO_FAILURE = 0xFFFFFFFFFFFFFFFF
+J2_NDIAG = 22
+
+
+class J2VPMaterialC(ctypes.Structure):
+    """``cib_j2vp_material``."""
+
+    _fields_ = [
+        ("young_modulus", ctypes.c_double),
+        ("poisson_ratio", ctypes.c_double),
+        ("yield_stress", ctypes.c_double),
+        ("hardening_modulus", ctypes.c_double),
+        ("time_scale", ctypes.c_double),
+        ("reference_stress", ctypes.c_double),
+        ("rate_exponent", ctypes.c_double),
+    ]
+
+
+class UpdateSettingsC(ctypes.Structure):
+    """``cib_update_settings``."""
+
+    _fields_ = [
+        ("max_iterations", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("yield_relative_tolerance", ctypes.c_double),
+        ("residual_absolute_tolerance", ctypes.c_double),
+        ("residual_relative_tolerance", ctypes.c_double),
+    ]
+
+
+class J2VPFailureC(ctypes.Structure):
+    """``cib_j2vp_failure``."""
+
+    _fields_ = [
+        ("reason", ctypes.c_int32),
+        ("iteration", ctypes.c_int32),
+        ("max_iterations", ctypes.c_int32),
+        ("algorithm", ctypes.c_int32),
+        ("time_step", ctypes.c_double),
+        ("shear_modulus", ctypes.c_double),
+        ("hardening_slope", ctypes.c_double),
+        ("trial_yield", ctypes.c_double),
+        ("physical_upper_bound", ctypes.c_double),
+        ("plastic_multiplier", ctypes.c_double),
+        ("corrected_overstress", ctypes.c_double),
+        ("residual", ctypes.c_double),
+        ("residual_tolerance", ctypes.c_double),
+        ("derivative", ctypes.c_double),
+        ("newton_candidate", ctypes.c_double),
+        ("radicand", ctypes.c_double),
+        ("yield_scale", ctypes.c_double),
+        ("yield_activation_threshold", ctypes.c_double),
+        ("trial_equivalent_stress", ctypes.c_double),
+        ("yield_radius", ctypes.c_double),
+        ("equivalent_plastic_strain", ctypes.c_double),
+        ("trial_stress", ctypes.c_double * 6),
+        ("deviatoric_stress", ctypes.c_double * 6),
+        ("has_residual", ctypes.c_int32),
+        ("has_derivative", ctypes.c_int32),
+        ("has_newton_candidate", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+    ]
+
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_I = ctypes.c_int
+
+# name -> (restype, argtypes); every symbol declared in include/cib200.h.
+SIGNATURES: dict[str, tuple[object, list[object]]] = {
+    "cib_j2vp_update_soa_f64": (_I, [_P, _P, _I64, _I64, _D] + [_P] * 10),
+    "cib_j2vp_update_soa_f32": (_I, [_P, _P, _I64, _I64, _D] + [_P] * 10),
+    "cib_j2vp_update": (_I, [_P, _P, _I64, _D] + [_P] * 16),
+    "cib_j2vp_diagnose_point": (_I, [_P, _P, _I64, _D, _P, _P, _P, _P, _I64, _P, _P]),
+    "cib_linear_elastic_update": (_I, [_D, _D, _I64, _D] + [_P] * 7),
+    "cib_copy_rows_async": (_I, [_P, _I64, _P, _I64, _I64, _I64, _I, _P]),
+    "cib_j2_diagnostic_name": (ctypes.c_char_p, [_I]),
+    "cib_j2_reason": (ctypes.c_char_p, [_I]),
+    "cib_last_cuda_error": (_I, []),
+    "cib_version": (ctypes.c_char_p, []),
+}
+
+_LIB: ctypes.CDLL | None = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Load ``libcib200.so`` and bind every declared symbol (raises if missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m concrete_impact_b200.build` "
+            "(this package has no CPU fallback)."
+        )
+    lib = ctypes.CDLL(os.fspath(LIB_PATH), mode=ctypes.RTLD_GLOBAL)
+    for name, (restype, argtypes) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    _LIB = lib
+    return lib
+
+
+def require_cuda() -> torch.device:
+    """Return the current CUDA device or raise: the kernels have no CPU path."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("concrete_impact_b200 kernels need a CUDA device (sm_100a); none is available.")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def ptr(tensor: torch.Tensor | None) -> int | None:
+    """Device pointer of a tensor (None passes NULL)."""
+    return None if tensor is None else tensor.data_ptr()
+
+
+def stream_ptr(stream: torch.cuda.Stream | None = None) -> int:
+    """Raw ``cudaStream_t`` of a torch stream (current stream by default)."""
+    stream = torch.cuda.current_stream() if stream is None else stream
+    return stream.cuda_stream
+
+
+def check(code: int, what: str) -> None:
+    """Raise on a non-zero return code of an entry point."""
+    if code != 0:
+        lib = load_library()
+        cuda = lib.cib_last_cuda_error()
+        raise RuntimeError(f"{what} failed with code {code} (last CUDA error {cuda}).")
+
+
+def j2_diagnostic_names() -> list[str]:
+    """Names of the diagnostic rows written by ``cib_j2vp_update``, in row order."""
+    lib = load_library()
+    return [lib.cib_j2_diagnostic_name(i).decode() for i in range(J2_NDIAG)]
+
+
+def j2_reason(code: int) -> str:
+    """Reference reason string of a per-point status code."""
+    return load_library().cib_j2_reason(code).decode()
+
+
+def material_struct(material) -> J2VPMaterialC:
+    """``cib_j2vp_material`` from a J2ViscoplasticMaterial-like object."""
+    return J2VPMaterialC(
+        float(material.young_modulus),
+        float(material.poisson_ratio),
+        float(material.yield_stress),
+        float(material.hardening_modulus),
+        float(material.time_scale),
+        float(material.reference_stress),
+        float(material.rate_exponent),
+    )
+
+
+def settings_struct(settings) -> UpdateSettingsC:
+    """``cib_update_settings`` from a MaterialUpdateSettings-like object."""
+    return UpdateSettingsC(
+        int(settings.max_iterations),
+        0,
+        float(settings.yield_relative_tolerance),
+        float(settings.residual_absolute_tolerance),
+        float(settings.residual_relative_tolerance),
+    )

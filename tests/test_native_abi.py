@@ -1,0 +1,89 @@
+"""CPU tests of the C ABI: the library loads and exports every symbol of include/cib200.h."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from concrete_impact_b200 import _native
+from concrete_impact_b200.materials import (
+    J2ViscoplasticMaterial,
+    MaterialPointRequest,
+    MaterialUpdateSettings,
+    build_j2_viscoplastic_material,
+)
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def _declared_functions() -> set[str]:
+    text = (REPO / "include" / "cib200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(cib_[a-z0-9_]+)\s*\(", text))
+
+
+def test_library_exports_every_declared_symbol() -> None:
+    lib = _native.load_library()
+    declared = _declared_functions()
+    assert declared, "no declarations parsed"
+    for name in sorted(declared):
+        assert hasattr(lib, name), name
+    # and nm agrees (dynamic symbol table, C linkage)
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_native.LIB_PATH)], capture_output=True, text=True, check=True)
+    exported = set(re.findall(r"\bT (cib_[a-z0-9_]+)$", out.stdout, flags=re.M))
+    assert declared <= exported, declared - exported
+    assert set(_native.SIGNATURES) == declared
+
+
+def test_struct_layouts_match_header() -> None:
+    """ctypes mirrors of the C structs have the C sizes (no silent padding mismatch)."""
+    assert ctypes.sizeof(_native.J2VPMaterialC) == 7 * 8
+    assert ctypes.sizeof(_native.UpdateSettingsC) == 8 + 3 * 8
+    assert ctypes.sizeof(_native.J2VPFailureC) == 16 + 17 * 8 + 12 * 8 + 16
+
+
+def test_names_and_reasons_need_no_gpu() -> None:
+    names = _native.j2_diagnostic_names()
+    from oracle.j2vp import DIAGNOSTIC_NAMES, REASONS
+
+    assert names == DIAGNOSTIC_NAMES
+    assert [_native.j2_reason(i) for i in range(len(REASONS))] == REASONS
+    assert _native.load_library().cib_version().decode().startswith("cib200")
+
+
+def test_argument_errors_are_rejected_without_a_launch() -> None:
+    lib = _native.load_library()
+    m = _native.J2VPMaterialC(25e9, 0.2, 20e6, 2e9, 1e-3, 20e6, 1.0)
+    s = _native.UpdateSettingsC(50, 0, 1e-10, 1e-12, 1e-10)
+    # null buffers and negative sizes come back as CIB_EINVAL (-1)
+    assert lib.cib_j2vp_update_soa_f64(ctypes.byref(m), ctypes.byref(s), 16, 16, 1e-5, *([None] * 10)) == -1
+    assert lib.cib_j2vp_update_soa_f64(ctypes.byref(m), ctypes.byref(s), -1, 0, 1e-5, *([None] * 10)) == -1
+    assert lib.cib_j2vp_update(ctypes.byref(m), ctypes.byref(s), 4, 1e-5, *([None] * 16)) == -1
+    assert lib.cib_copy_rows_async(None, 8, None, 8, 8, 1, 1, None) == -1
+    # zero points is a no-op success
+    assert lib.cib_j2vp_update_soa_f32(ctypes.byref(m), ctypes.byref(s), 0, 0, 1e-5, *([1] * 9), None, None, None) == 0
+
+
+def test_kinematics_and_shape_contract_errors_precede_the_gpu() -> None:
+    material = J2ViscoplasticMaterial("m", 1.0, 1000.0, 0.25, 1.0, 1.0, 1.0, 1.0, 1.0)
+    settings = MaterialUpdateSettings(50, 1e-10, 1e-12, 1e-10)
+    state = material.initialize_state(2)
+    with pytest.raises(ValueError, match="three_dimensional"):
+        material.update(MaterialPointRequest(np.zeros((2, 6)), None, 1.0, "plane_strain", settings), state)
+    with pytest.raises(ValueError, match=r"\(n_points, 6\)"):
+        material.update(MaterialPointRequest(np.zeros((2, 3)), None, 1.0, "three_dimensional", settings), state)
+
+
+def test_material_validation_matches_reference_messages() -> None:
+    base = dict(name="m", density=1.0, young_modulus=1.0, poisson_ratio=0.2, yield_stress=1.0, hardening_modulus=0.0,
+                time_scale=1.0, reference_stress=1.0, rate_exponent=1.0)  # fmt: skip
+    build_j2_viscoplastic_material(base)
+    for key, value, message in [("young_modulus", 0.0, "young_modulus > 0"), ("poisson_ratio", 0.5, "poisson_ratio"),
+                                ("rate_exponent", 0.5, "rate_exponent >= 1"), ("time_scale", 0.0, "time_scale > 0")]:  # fmt: skip
+        with pytest.raises(ValueError, match=message):
+            build_j2_viscoplastic_material({**base, key: value})
