@@ -184,11 +184,12 @@ def test_loading_diagnostics_separate_work_stress_and_flow() -> None:
     material = _test_material(2.0, 0.02)
     loaded_strain = np.zeros(6)
     loaded_strain[5] = 0.02
-    loaded = material.update(_request(loaded_strain, 1e-3, np.zeros((1, 6))), material.initialize_state(1), FULL)
+    rate = (loaded_strain / 1e-3).reshape(1, 6)  # step-average rate from a zero previous strain
+    loaded = material.update(_request(loaded_strain, 1e-3, rate), material.initialize_state(1), FULL)
     assert loaded.diagnostics["incremental_work_density"][0] > 0.0
     assert loaded.diagnostics["equivalent_stress_increment"][0] > 0.0
     assert loaded.diagnostics["viscoplastic_active"][0] == 1.0
-    relaxed = material.update(_request(loaded_strain, 1e-3, loaded_strain.reshape(1, 6)), loaded.state, FULL)
+    relaxed = material.update(_request(loaded_strain, 1e-3, np.zeros((1, 6))), loaded.state, FULL)
     assert relaxed.diagnostics["incremental_work_density"][0] == pytest.approx(0.0)
     assert relaxed.diagnostics["equivalent_stress_increment"][0] < 0.0
     assert relaxed.diagnostics["viscoplastic_active"][0] == 1.0
