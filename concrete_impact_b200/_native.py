@@ -78,6 +78,57 @@ class J2VPFailureC(ctypes.Structure):
     ]
 
 
+class RVEDescC(ctypes.Structure):
+    """``cib_rve_desc``."""
+
+    _fields_ = [
+        ("nx", ctypes.c_int32),
+        ("ny", ctypes.c_int32),
+        ("nz", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("elem_offset", ctypes.c_int64),
+        ("hx", ctypes.c_double),
+        ("hy", ctypes.c_double),
+        ("hz", ctypes.c_double),
+    ]
+
+
+class PhaseMaterialC(ctypes.Structure):
+    """``cib_phase_material``."""
+
+    _fields_ = [("kind", ctypes.c_int32), ("pad_", ctypes.c_int32), ("params", J2VPMaterialC)]
+
+
+RVE_MAX_PHASES = 8
+
+
+class RVEBatchC(ctypes.Structure):
+    """``cib_rve_batch``."""
+
+    _fields_ = [
+        ("nrve", ctypes.c_int32),
+        ("nphase", ctypes.c_int32),
+        ("nelem", ctypes.c_int64),
+        ("precision", ctypes.c_int32),
+        ("max_nxy", ctypes.c_int32),
+        ("desc", ctypes.c_void_p),
+        ("phase", ctypes.c_void_p),
+        ("mats", PhaseMaterialC * RVE_MAX_PHASES),
+        ("settings", UpdateSettingsC),
+        ("plastic_strain_n", ctypes.c_void_p),
+        ("eqps_n", ctypes.c_void_p),
+        ("vpm_n", ctypes.c_void_p),
+        ("plastic_strain", ctypes.c_void_p),
+        ("eqps", ctypes.c_void_p),
+        ("vpm", ctypes.c_void_p),
+        ("stress", ctypes.c_void_p),
+        ("tparam", ctypes.c_void_p),
+        ("tflag", ctypes.c_void_p),
+        ("fe", ctypes.c_void_p),
+        ("de", ctypes.c_void_p),
+    ]
+
+
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
 _D = ctypes.c_double
@@ -91,6 +142,12 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_j2vp_diagnose_point": (_I, [_P, _P, _I64, _D, _P, _P, _P, _P, _I64, _P, _P]),
     "cib_linear_elastic_update": (_I, [_D, _D, _I64, _D] + [_P] * 7),
     "cib_copy_rows_async": (_I, [_P, _I64, _P, _I64, _I64, _I64, _I, _P]),
+    "cib_rve_residual": (_I, [_P] * 9),
+    "cib_rve_gather": (_I, [_P] * 12),
+    "cib_rve_pcg": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32] + [_P] * 5),
+    "cib_rve_tangent_rhs": (_I, [_P] * 6),
+    "cib_rve_tangent_finish": (_I, [_P] * 7),
+    "cib_rve_response": (_I, [_P] * 11),
     "cib_j2_diagnostic_name": (ctypes.c_char_p, [_I]),
     "cib_j2_reason": (ctypes.c_char_p, [_I]),
     "cib_last_cuda_error": (_I, []),

@@ -1,0 +1,1080 @@
+// Periodic structured Hex8 RVE kernels (sm_100a): fused residual, deterministic periodic
+// gather, matrix-free PCG, homogenisation.
+//
+// Restates, for structured periodic boxes, the reference's
+//   _compute_hex8_strain_fields + material update + _assemble_force_and_tangent
+//       (src/fem/assembly/nonlinear_solid.py:428-493) -- fused into rve_residual_kernel;
+//   u = T w + A ebar and r = T^T f_int (src/fem/rve/solver.py:88-100, periodic.py:20-169);
+//   the reduced solve K_red dw = -r (solver.py:143-144), done here by Jacobi-PCG with a
+//       matrix-free tangent apply instead of SuperLU;
+//   the homogenisation and diagnostics of _build_rve_response (solver.py:253-364);
+//   the Schur-complement effective tangent (solver.py:438-461) via multi-RHS PCG.
+//
+// Layout.  Batch of R RVEs; RVE r has nx*ny*nz elements starting at element eoff; its
+// periodic node (equivalence class) c = i + nx (j + ny k) is stored at batch node eoff + c,
+// so classes and elements share offsets.  Class 0 is the eliminated reference class (its
+// entries stay zero).  Gauss-point arrays are SoA over all 8 E points of the batch; GP q
+// of element e is point 8 e + q, q = 4 a + 2 b + c for the Gauss coordinates
+// (xi_a, eta_b, zeta_c) (itertools.product order, quadrature/rules.py:24-33).  Element
+// node a has signs (a&1, a&2, a&4) -> lexicographic order of elements/lagrange.py:50-76.
+//
+// Parallel mapping.  One CTA per RVE (or per linear system): every reduction is CTA-local
+// and in a fixed order, so results are bitwise reproducible.  Within a CTA, one thread per
+// Gauss point; the 8 threads of an element exchange nodal values with warp shuffles and
+// reduce-scatter their B^T sigma contributions so that thread q ends with element node q.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cib_common.cuh"
+#include "j2vp_point.cuh"
+#include "rve.cuh"
+
+namespace cib {
+
+namespace {
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// Reference-element gradient dN_a/dxi_d at Gauss point q (before the 2/h scaling).
+__device__ __forceinline__ void ref_grad(int q, int a, double g[3]) {
+  const double gp = 0.57735026918962576451;  // 1/sqrt(3)
+  const double xi = (q & 4) ? gp : -gp;
+  const double eta = (q & 2) ? gp : -gp;
+  const double zeta = (q & 1) ? gp : -gp;
+  const double sx = (a & 1) ? 1.0 : -1.0, sy = (a & 2) ? 1.0 : -1.0, sz = (a & 4) ? 1.0 : -1.0;
+  const double fx = 1.0 + sx * xi, fy = 1.0 + sy * eta, fz = 1.0 + sz * zeta;
+  g[0] = 0.125 * sx * fy * fz;
+  g[1] = 0.125 * sy * fx * fz;
+  g[2] = 0.125 * sz * fx * fy;
+}
+
+template <typename T>
+struct Grad8 {
+  T x[8], y[8], z[8];
+};
+
+template <typename T>
+__device__ __forceinline__ void physical_grads(int q, const RveDesc& d, Grad8<T>& G) {
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double g[3];
+    ref_grad(q, a, g);
+    G.x[a] = (T)(g[0] * 2.0 / d.hx);
+    G.y[a] = (T)(g[1] * 2.0 / d.hy);
+    G.z[a] = (T)(g[2] * 2.0 / d.hz);
+  }
+}
+
+// eps = B u for the 24 nodal values u[a][d] (Voigt xx,yy,zz,yz,xz,xy; engineering shear).
+template <typename T>
+__device__ __forceinline__ void strain_from(const Grad8<T>& G, const T u[8][3], T e[6]) {
+  T exx = 0, eyy = 0, ezz = 0, gyz = 0, gxz = 0, gxy = 0;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    exx += G.x[a] * u[a][0];
+    eyy += G.y[a] * u[a][1];
+    ezz += G.z[a] * u[a][2];
+    gyz += G.z[a] * u[a][1] + G.y[a] * u[a][2];
+    gxz += G.z[a] * u[a][0] + G.x[a] * u[a][2];
+    gxy += G.y[a] * u[a][0] + G.x[a] * u[a][1];
+  }
+  e[0] = exx;
+  e[1] = eyy;
+  e[2] = ezz;
+  e[3] = gyz;
+  e[4] = gxz;
+  e[5] = gxy;
+}
+
+// f[a][d] = w * (B_a^T s)_d
+template <typename T>
+__device__ __forceinline__ void bt_stress(const Grad8<T>& G, const T s[6], T w, T f[8][3]) {
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    f[a][0] = w * (G.x[a] * s[0] + G.z[a] * s[4] + G.y[a] * s[5]);
+    f[a][1] = w * (G.y[a] * s[1] + G.z[a] * s[3] + G.x[a] * s[5]);
+    f[a][2] = w * (G.z[a] * s[2] + G.y[a] * s[3] + G.x[a] * s[4]);
+  }
+}
+
+// Gauss point tangent: tau = C eps, for an elastic phase (params unused) or a J2 point with
+// tangent parameters (n[6], f, c, active flag encoded by c/f).
+template <typename T>
+struct TangentParams {
+  T n[6];
+  T f;
+  T c;
+  int elastic;  // 1: use the elasticity matrix of the phase
+};
+
+template <typename T>
+__device__ __forceinline__ void tangent_apply(const PhaseMat<T>& m, const TangentParams<T>& tp, const T e[6],
+                                              T s[6]) {
+  if (tp.elastic) {
+    s[0] = m.C11 * e[0] + m.C12 * e[1] + m.C12 * e[2];
+    s[1] = m.C12 * e[0] + m.C11 * e[1] + m.C12 * e[2];
+    s[2] = m.C12 * e[0] + m.C12 * e[1] + m.C11 * e[2];
+    s[3] = m.G * e[3];
+    s[4] = m.G * e[4];
+    s[5] = m.G * e[5];
+    return;
+  }
+  const T tr = e[0] + e[1] + e[2];
+  const T ne = tp.n[0] * e[0] + tp.n[1] * e[1] + tp.n[2] * e[2] + tp.n[3] * e[3] + tp.n[4] * e[4] + tp.n[5] * e[5];
+  const T vol = m.K * tr;
+  const T third = tr * (T)(1.0 / 3.0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) s[i] = vol + tp.f * (e[i] - third) + tp.c * tp.n[i] * ne;
+#pragma unroll
+  for (int i = 3; i < 6; ++i) s[i] = (T)0.5 * tp.f * e[i] + tp.c * tp.n[i] * ne;
+}
+
+// Butterfly reduce-scatter of 24 values over the 8 lanes of an element group: on return,
+// out[0..2] of lane q holds the sum over the group of v[3q .. 3q+2].
+template <typename T>
+__device__ __forceinline__ void reduce_scatter8(const T (&v)[8][3], int q, T out[3]) {
+  T h[4][3];  // after xor 4: nodes (q&4) .. (q&4)+3
+#pragma unroll
+  for (int t = 0; t < 4; ++t)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const T send = (q & 4) ? v[t][d] : v[t + 4][d];
+      const T keep = (q & 4) ? v[t + 4][d] : v[t][d];
+      h[t][d] = keep + __shfl_xor_sync(FULL_MASK, send, 4);
+    }
+  T g[2][3];  // after xor 2: nodes (q&6), (q&6)+1
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const T send = (q & 2) ? h[t][d] : h[t + 2][d];
+      const T keep = (q & 2) ? h[t + 2][d] : h[t][d];
+      g[t][d] = keep + __shfl_xor_sync(FULL_MASK, send, 2);
+    }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const T send = (q & 1) ? g[0][d] : g[1][d];
+    const T keep = (q & 1) ? g[1][d] : g[0][d];
+    out[d] = keep + __shfl_xor_sync(FULL_MASK, send, 1);
+  }
+}
+
+// Broadcast the 3 nodal values held by each lane of the 8-lane group to all of them.
+template <typename T>
+__device__ __forceinline__ void allgather8(const T mine[3], T u[8][3]) {
+  const int base = (threadIdx.x & 31) & ~7;
+#pragma unroll
+  for (int b = 0; b < 8; ++b)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[b][d] = __shfl_sync(FULL_MASK, mine[d], base + b);
+}
+
+__device__ __forceinline__ int64_t periodic_node(const RveDesc& d, int i, int j, int k) {
+  i %= d.nx;
+  j %= d.ny;
+  k %= d.nz;
+  return d.eoff + i + (int64_t)d.nx * (j + (int64_t)d.ny * k);
+}
+
+// Node a of local element (i, j, k): periodic batch node.
+__device__ __forceinline__ int64_t element_node(const RveDesc& d, int i, int j, int k, int a) {
+  return periodic_node(d, i + (a & 1), j + ((a >> 1) & 1), k + ((a >> 2) & 1));
+}
+
+__device__ __forceinline__ void local_ijk(const RveDesc& d, int64_t le, int& i, int& j, int& k) {
+  i = (int)(le % d.nx);
+  j = (int)((le / d.nx) % d.ny);
+  k = (int)(le / ((int64_t)d.nx * d.ny));
+}
+
+// CTA-wide sum of NV doubles (fixed order: warp tree, then warp 0 over warps).
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch /* >= 32 * NV */) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(FULL_MASK, v[k], o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) scratch[warp * NV + k] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double x = lane < nw ? scratch[lane * NV + k] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
+      v[k] = x;
+    }
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) scratch[k] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = scratch[k];
+  __syncthreads();
+}
+
+__device__ __forceinline__ double block_max(double v, double* scratch) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL_MASK, v, o));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double x = lane < nw ? scratch[lane] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(FULL_MASK, x, o));
+    if (lane == 0) scratch[0] = x;
+  }
+  __syncthreads();
+  v = scratch[0];
+  __syncthreads();
+  return v;
+}
+
+__device__ __forceinline__ double block_min(double v, double* scratch) { return -block_max(-v, scratch); }
+
+// Current fluctuation at a batch node: w_base + alpha * dw (dw may be null).
+__device__ __forceinline__ void load_w(const double* w, const double* dw, double alpha, int64_t node, double out[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double v = w[3 * node + d];
+    if (dw) v += alpha * dw[3 * node + d];
+    out[d] = v;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// Fused residual: strains, return map, trial state, tangent parameters, element nodal
+// forces and Jacobi diagonal contributions.  One CTA per RVE.
+template <typename T>
+__global__ void __launch_bounds__(RVE_THREADS) rve_residual_kernel(const RveResidualArgs<T> a) {
+  const int r = blockIdx.x;
+  if (a.active && !a.active[r]) return;
+  const RveDesc d = a.desc[r];
+  const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+  const int64_t G = 8 * E;
+  const double alpha = a.alpha ? a.alpha[r] : 1.0;
+  T ebar[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ebar[k] = (T)a.macro[6 * r + k];
+  const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
+  const int64_t rounds = (G + blockDim.x - 1) / blockDim.x;
+  for (int64_t it = 0; it < rounds; ++it) {
+    const int64_t gl = it * blockDim.x + threadIdx.x;
+    const bool live = gl < G;  // whole 8-lane groups are live or not (G, blockDim multiples of 8)
+    const int64_t le = live ? (gl >> 3) : 0;
+    const int q = (int)(gl & 7);
+    int i, j, k;
+    local_ijk(d, le, i, j, k);
+    const int64_t e = d.eoff + le;
+    const int64_t g = 8 * e + q;
+    double wq[3] = {0.0, 0.0, 0.0};
+    if (live) load_w(a.w, a.dw, alpha, element_node(d, i, j, k, q), wq);
+    T mine[3] = {(T)wq[0], (T)wq[1], (T)wq[2]};
+    T u[8][3];
+    allgather8(mine, u);
+    Grad8<T> Gr;
+    physical_grads(q, d, Gr);
+    T eps[6];
+    strain_from(Gr, u, eps);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) eps[c] += ebar[c];
+    const int ph = live ? (int)a.phase[e] : 0;
+    const PhaseMat<T>& m = a.mats.m[ph];
+    T sig[6];
+    TangentParams<T> tp;
+    tp.elastic = 1;
+    tp.f = (T)0;
+    tp.c = (T)0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tp.n[c] = (T)0;
+    if (live) {
+      if (m.kind == PHASE_J2VP) {
+        T ep[6], eel[6], st[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          ep[c] = a.ep_n[c * a.ngp + g];
+          eel[c] = eps[c] - ep[c];
+        }
+        elastic_stress(m.j2, eel, st);
+        const double qn = a.q_n[g];
+        J2Out<T> o;
+        const int status = j2vp_point<T, false>(m.j2, (T)a.dt[r], st, qn, o);
+        if (status != CIB_J2_OK) {
+          if (a.fail) atomicMin(&a.fail[r], (unsigned long long)(8 * le + q));
+#pragma unroll
+          for (int c = 0; c < 6; ++c) o.sigma[c] = st[c];
+          o.active = 0;
+          o.dgamma = (T)0;
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          sig[c] = o.sigma[c];
+          a.ep[c * a.ngp + g] = ep[c] + (c < 3 ? o.dgamma : (T)2 * o.dgamma) * (o.active ? o.n[c] : (T)0);
+        }
+        a.q[g] = qn + (double)o.dgamma;
+        a.vpm[g] = a.vpm_n[g] + (double)o.dgamma;
+        if (o.active) {
+          tp.elastic = 0;
+          tp.f = o.tan_f;
+          tp.c = o.tan_c;
+#pragma unroll
+          for (int c = 0; c < 6; ++c) tp.n[c] = o.n[c];
+        }
+      } else {
+        elastic_stress(m.j2, eps, sig);
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        a.stress[c * a.ngp + g] = sig[c];
+        a.tparam[c * a.ngp + g] = tp.n[c];
+      }
+      a.tparam[6 * a.ngp + g] = tp.f;
+      a.tparam[7 * a.ngp + g] = tp.elastic ? (T)0 : tp.c;
+      a.tflag[g] = (uint8_t)(tp.elastic ? 0 : 1);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) sig[c] = (T)0;
+    }
+    // Element nodal forces w_q B_q^T sigma_q and Jacobi diagonal contributions.
+    T f[8][3];
+    bt_stress(Gr, sig, jw, f);
+    T diag[8][3];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) {
+        T ec[6] = {0, 0, 0, 0, 0, 0};
+        // B column of (node b, direction dd)
+        if (dd == 0) {
+          ec[0] = Gr.x[b];
+          ec[4] = Gr.z[b];
+          ec[5] = Gr.y[b];
+        } else if (dd == 1) {
+          ec[1] = Gr.y[b];
+          ec[3] = Gr.z[b];
+          ec[5] = Gr.x[b];
+        } else {
+          ec[2] = Gr.z[b];
+          ec[3] = Gr.y[b];
+          ec[4] = Gr.x[b];
+        }
+        T sc[6];
+        tangent_apply(m, tp, ec, sc);
+        diag[b][dd] = live ? jw * (ec[0] * sc[0] + ec[1] * sc[1] + ec[2] * sc[2] + ec[3] * sc[3] + ec[4] * sc[4] +
+                                   ec[5] * sc[5])
+                           : (T)0;
+      }
+    }
+    T fo[3], dgo[3];
+    reduce_scatter8(f, q, fo);
+    reduce_scatter8(diag, q, dgo);
+    if (live) {
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) {
+        a.fe[(8 * e + q) * 3 + dd] = (double)fo[dd];
+        a.de[(8 * e + q) * 3 + dd] = (double)dgo[dd];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Periodic gather: reduced residual r = T^T f (class 0 removed), Jacobi inverse diagonal,
+// squared norm, class-reaction maximum (class 0 included) and, optionally, the
+// materialised trial fluctuation w_out = w + alpha dw.  One CTA per RVE.
+__global__ void __launch_bounds__(RVE_THREADS) rve_gather_kernel(const RveGatherArgs a) {
+  __shared__ double scratch[32 * 2];
+  const int r = blockIdx.x;
+  if (a.active && !a.active[r]) return;
+  const RveDesc d = a.desc[r];
+  const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+  const double alpha = a.alpha ? a.alpha[r] : 1.0;
+  double acc[2] = {0.0, 0.0};  // ||r||^2, ||w + alpha dw||^2
+  double cmax = 0.0;
+  for (int64_t c = threadIdx.x; c < E; c += blockDim.x) {
+    int i, j, k;
+    local_ijk(d, c, i, j, k);
+    double f[3] = {0.0, 0.0, 0.0}, dg[3] = {0.0, 0.0, 0.0};
+    for (int n = 0; n < 8; ++n) {
+      const int di = n & 1, dj = (n >> 1) & 1, dk = (n >> 2) & 1;
+      const int ie = (i - di + d.nx) % d.nx, je = (j - dj + d.ny) % d.ny, ke = (k - dk + d.nz) % d.nz;
+      const int64_t e = d.eoff + ie + (int64_t)d.nx * (je + (int64_t)d.ny * ke);
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) {
+        f[dd] += a.fe[(8 * e + n) * 3 + dd];
+        dg[dd] += a.de[(8 * e + n) * 3 + dd];
+      }
+    }
+    const int64_t node = d.eoff + c;
+    cmax = fmax(cmax, sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]));
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      const bool fixed = (c == 0);
+      a.res[3 * node + dd] = fixed ? 0.0 : f[dd];
+      a.dinv[3 * node + dd] = fixed ? 0.0 : 1.0 / dg[dd];
+      if (!fixed) acc[0] += f[dd] * f[dd];
+    }
+    double w[3];
+    load_w(a.w, a.dw, alpha, node, w);
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      const double wv = (c == 0) ? 0.0 : w[dd];
+      acc[1] += wv * wv;
+      if (a.w_out) a.w_out[3 * node + dd] = wv;
+    }
+  }
+  block_sum<2>(acc, scratch);
+  cmax = block_max(cmax, scratch);
+  if (threadIdx.x == 0) {
+    a.rnorm2[r] = acc[0];
+    if (a.wnorm2) a.wnorm2[r] = acc[1];
+    if (a.class_max) a.class_max[r] = cmax;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Matrix-free apply of the reduced tangent to one periodic vector, streaming the RVE in
+// z-layers: element results of a layer go to shared memory, then every node of the layer
+// gathers its 4 bottom and 4 top contributions in a fixed order.  Returns p . Ap (CTA-wide).
+template <typename T>
+__device__ double apply_tangent(const RvePcgArgs<T>& a, const RveDesc& d, const double* __restrict__ p,
+                                double* __restrict__ Ap, double* smem, double* scratch) {
+  const int nxy = d.nx * d.ny;
+  double* ye = smem;                  // nxy * 24
+  double* acc_cur = ye + 24 * nxy;    // nxy * 3
+  double* acc_next = acc_cur + 3 * nxy;
+  double* acc_first = acc_next + 3 * nxy;
+  const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
+  double pap[1] = {0.0};
+  const int items = 8 * nxy;
+  const int rounds = (items + blockDim.x - 1) / blockDim.x;
+  for (int k = 0; k < d.nz; ++k) {
+    for (int it = 0; it < rounds; ++it) {
+      const int gl = it * blockDim.x + threadIdx.x;
+      const bool live = gl < items;
+      const int el = live ? (gl >> 3) : 0;
+      const int q = gl & 7;
+      const int i = el % d.nx, j = el / d.nx;
+      const int64_t e = d.eoff + el + (int64_t)nxy * k;
+      T mine[3] = {0, 0, 0};
+      if (live) {
+        const int64_t node = element_node(d, i, j, k, q);
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) mine[dd] = (T)p[3 * node + dd];
+      }
+      T u[8][3];
+      allgather8(mine, u);
+      Grad8<T> Gr;
+      physical_grads(q, d, Gr);
+      T eps[6], sig[6];
+      strain_from(Gr, u, eps);
+      const int64_t g = 8 * e + q;
+      const int ph = live ? (int)a.phase[e] : 0;
+      TangentParams<T> tp;
+      tp.elastic = 1;
+      tp.f = (T)0;
+      tp.c = (T)0;
+      if (live && a.tflag[g]) {
+        tp.elastic = 0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) tp.n[c] = a.tparam[c * a.ngp + g];
+        tp.f = a.tparam[6 * a.ngp + g];
+        tp.c = a.tparam[7 * a.ngp + g];
+      }
+      tangent_apply(a.mats.m[ph], tp, eps, sig);
+      T f[8][3];
+      bt_stress(Gr, sig, live ? jw : (T)0, f);
+      T out[3];
+      reduce_scatter8(f, q, out);
+      if (live)
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) ye[(8 * el + q) * 3 + dd] = (double)out[dd];
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
+      const int i = n % d.nx, j = n / d.nx;
+      double bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
+      for (int s = 0; s < 4; ++s) {
+        const int di = s & 1, dj = s >> 1;
+        const int el = (i - di + d.nx) % d.nx + d.nx * ((j - dj + d.ny) % d.ny);
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+          bot[dd] += ye[(8 * el + s) * 3 + dd];
+          top[dd] += ye[(8 * el + s + 4) * 3 + dd];
+        }
+      }
+      if (k == 0) {
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) acc_first[3 * n + dd] = bot[dd];
+      } else {
+        const int64_t node = d.eoff + n + (int64_t)nxy * k;
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+          const double v = acc_cur[3 * n + dd] + bot[dd];
+          Ap[3 * node + dd] = v;
+          pap[0] += p[3 * node + dd] * v;
+        }
+      }
+      if (k == d.nz - 1) {
+        const int64_t node = d.eoff + n;
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+          const double v = (n == 0) ? 0.0 : acc_first[3 * n + dd] + top[dd];
+          Ap[3 * node + dd] = v;
+          pap[0] += p[3 * node + dd] * v;
+        }
+      } else {
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) acc_next[3 * n + dd] = top[dd];
+      }
+    }
+    __syncthreads();
+    double* t = acc_cur;
+    acc_cur = acc_next;
+    acc_next = t;
+  }
+  block_sum<1>(pap, scratch);
+  return pap[0];
+}
+
+// Jacobi-PCG on one reduced periodic system per CTA: K x = b, x0 = 0.  Bounded iterations;
+// status 0 converged (||r|| <= rtol ||b|| or ||b|| == 0), 1 iteration limit, 2 breakdown
+// (p.Ap <= 0 or non-finite).
+template <typename T>
+__global__ void __launch_bounds__(RVE_THREADS) rve_pcg_kernel(const RvePcgArgs<T> a) {
+  extern __shared__ double smem[];
+  __shared__ double scratch[64];
+  const int s = blockIdx.x;
+  const int r = a.sys_rve[s];
+  if (a.active && !a.active[r]) return;
+  const RveDesc d = a.desc[r];
+  const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+  const int64_t off = a.sys_off[s];  // vector offset of this system (3 * node base)
+  const double* b = a.b + off;
+  double* x = a.x + off;
+  double* rr = a.r + off;
+  double* p = a.p + off;
+  double* Ap = a.Ap + off;
+  const double* dinv = a.dinv + 3 * d.eoff;
+  // Shift the vector pointers so that batch node indices address them directly.
+  const int64_t shift = 3 * d.eoff;
+  double* x_ = x - shift;
+  double* r_ = rr - shift;
+  double* p_ = p - shift;
+  double* Ap_ = Ap - shift;
+  double v[2] = {0.0, 0.0};  // rz, bb
+  for (int64_t n = threadIdx.x; n < 3 * E; n += blockDim.x) {
+    const double bi = b[n];
+    x[n] = 0.0;
+    rr[n] = bi;
+    const double z = dinv[n] * bi;
+    p[n] = z;
+    v[0] += bi * z;
+    v[1] += bi * bi;
+  }
+  block_sum<2>(v, scratch);
+  double rz = v[0];
+  const double bnorm = sqrt(v[1]);
+  const double tol = a.rtol * bnorm;
+  int status = 1, iters = 0;
+  double rnorm = bnorm;
+  if (bnorm == 0.0 || !(bnorm == bnorm)) {
+    status = (bnorm == 0.0) ? 0 : 2;
+  } else {
+    for (iters = 0; iters < a.maxit;) {
+      const double pap = apply_tangent<T>(a, d, p_, Ap_, smem, scratch);
+      if (!(pap > 0.0) || !isfinite(pap)) {
+        status = 2;
+        break;
+      }
+      const double alpha = rz / pap;
+      double w2[2] = {0.0, 0.0};  // r.r, r.z
+      for (int64_t n = threadIdx.x; n < 3 * E; n += blockDim.x) {
+        x[n] += alpha * p[n];
+        const double rn = rr[n] - alpha * Ap[n];
+        rr[n] = rn;
+        w2[0] += rn * rn;
+        w2[1] += rn * dinv[n] * rn;
+      }
+      block_sum<2>(w2, scratch);
+      ++iters;
+      rnorm = sqrt(w2[0]);
+      if (!isfinite(rnorm)) {
+        status = 2;
+        break;
+      }
+      if (rnorm <= tol) {
+        status = 0;
+        break;
+      }
+      const double beta = w2[1] / rz;
+      rz = w2[1];
+      for (int64_t n = threadIdx.x; n < 3 * E; n += blockDim.x) p[n] = dinv[n] * rr[n] + beta * p[n];
+      __syncthreads();
+    }
+  }
+  double xn[1] = {0.0};
+  for (int64_t n = threadIdx.x; n < 3 * E; n += blockDim.x) xn[0] += x[n] * x[n];
+  block_sum<1>(xn, scratch);
+  if (threadIdx.x == 0) {
+    a.status[s] = status;
+    a.iterations[s] = iters;
+    a.rel_residual[s] = bnorm > 0.0 ? rnorm / bnorm : 0.0;
+    a.xnorm[s] = sqrt(xn[0]);
+  }
+  (void)x_;
+  (void)r_;
+}
+
+// ---------------------------------------------------------------------------------------
+// Right-hand sides of the effective-tangent solves and K_ee.  For macro strain unit j,
+// element forces f_e^(j) = sum_q w B_q^T C_q e_j; gathered periodically they give column j
+// of K_we = T^T K A; K_ee = A^T K A = sum_q w C_q (since B_q A e_j = e_j on a box).
+// One CTA per RVE; rhs is (6, 3E) per RVE at offset 18 * eoff; kee is (R, 36).
+template <typename T>
+__global__ void __launch_bounds__(RVE_THREADS) rve_tangent_rhs_kernel(const RveTangentArgs<T> a) {
+  __shared__ double scratch[32 * 36];
+  const int r = blockIdx.x;
+  if (a.active && !a.active[r]) return;
+  const RveDesc d = a.desc[r];
+  const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+  const int64_t G = 8 * E;
+  const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
+  double kee[36];
+#pragma unroll
+  for (int t = 0; t < 36; ++t) kee[t] = 0.0;
+  const int64_t rounds = (G + blockDim.x - 1) / blockDim.x;
+  for (int64_t it = 0; it < rounds; ++it) {
+    const int64_t gl = it * blockDim.x + threadIdx.x;
+    const bool live = gl < G;
+    const int64_t le = live ? (gl >> 3) : 0;
+    const int q = (int)(gl & 7);
+    const int64_t e = d.eoff + le;
+    const int64_t g = 8 * e + q;
+    Grad8<T> Gr;
+    physical_grads(q, d, Gr);
+    const int ph = live ? (int)a.phase[e] : 0;
+    TangentParams<T> tp;
+    tp.elastic = 1;
+    tp.f = (T)0;
+    tp.c = (T)0;
+    if (live && a.tflag[g]) {
+      tp.elastic = 0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) tp.n[c] = a.tparam[c * a.ngp + g];
+      tp.f = a.tparam[6 * a.ngp + g];
+      tp.c = a.tparam[7 * a.ngp + g];
+    }
+#pragma unroll 1
+    for (int jcol = 0; jcol < 6; ++jcol) {
+      T ej[6] = {0, 0, 0, 0, 0, 0};
+      ej[jcol] = (T)1;
+      T sc[6];
+      tangent_apply(a.mats.m[ph], tp, ej, sc);
+      if (live)
+#pragma unroll
+        for (int i = 0; i < 6; ++i) kee[6 * i + jcol] += (double)jw * (double)sc[i];
+      T f[8][3];
+      bt_stress(Gr, sc, live ? jw : (T)0, f);
+      T out[3];
+      reduce_scatter8(f, q, out);
+      if (live)
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) a.fe6[((int64_t)jcol * a.ne_total * 8 + 8 * e + q) * 3 + dd] = (double)out[dd];
+    }
+  }
+  block_sum<36>(kee, scratch);
+  if (threadIdx.x == 0)
+    for (int t = 0; t < 36; ++t) a.kee[36 * r + t] = kee[t];
+  __syncthreads();
+  // Periodic gather of the 6 columns into rhs (class 0 removed).
+  for (int64_t c = threadIdx.x; c < E; c += blockDim.x) {
+    int i, j, k;
+    local_ijk(d, c, i, j, k);
+    for (int jcol = 0; jcol < 6; ++jcol) {
+      double f[3] = {0.0, 0.0, 0.0};
+      for (int n = 0; n < 8; ++n) {
+        const int di = n & 1, dj = (n >> 1) & 1, dk = (n >> 2) & 1;
+        const int ie = (i - di + d.nx) % d.nx, je = (j - dj + d.ny) % d.ny, ke = (k - dk + d.nz) % d.nz;
+        const int64_t e = d.eoff + ie + (int64_t)d.nx * (je + (int64_t)d.ny * ke);
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) f[dd] += a.fe6[((int64_t)jcol * a.ne_total * 8 + 8 * e + n) * 3 + dd];
+      }
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) a.rhs[18 * d.eoff + (int64_t)jcol * 3 * E + 3 * c + dd] = (c == 0) ? 0.0 : f[dd];
+    }
+  }
+}
+
+// C_eff = (K_ee - K_we^T S) / V, with S the 6 PCG solutions (same layout as rhs).
+__global__ void __launch_bounds__(RVE_THREADS) rve_tangent_finish_kernel(const RveTangentFinishArgs a) {
+  __shared__ double scratch[32 * 36];
+  const int r = blockIdx.x;
+  if (a.active && !a.active[r]) return;
+  const RveDesc d = a.desc[r];
+  const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+  double acc[36];
+#pragma unroll
+  for (int t = 0; t < 36; ++t) acc[t] = 0.0;
+  const double* rhs = a.rhs + 18 * d.eoff;
+  const double* sol = a.sol + 18 * d.eoff;
+  for (int64_t n = threadIdx.x; n < 3 * E; n += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      const double ki = rhs[i * 3 * E + n];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) acc[6 * i + j] += ki * sol[j * 3 * E + n];
+    }
+  }
+  block_sum<36>(acc, scratch);
+  if (threadIdx.x == 0) {
+    const double vol = d.hx * d.hy * d.hz * (double)E;
+    for (int t = 0; t < 36; ++t) a.ceff[36 * r + t] = (a.kee[36 * r + t] - acc[t]) / vol;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Response pass: homogenised stress, energies, work/activity statistics, phase averages,
+// virtual-work, periodicity and reaction diagnostics (solver.py:253-364, 464-494), and
+// optionally the per-point strains, strain rates, free energy, dissipation and the J2
+// diagnostics rows.  One CTA per RVE.
+template <typename T>
+__global__ void __launch_bounds__(RVE_THREADS) rve_response_kernel(const RveResponseArgs<T> a) {
+  __shared__ double scratch[32 * RVE_NSUM];
+  const int r = blockIdx.x;
+  if (a.active && !a.active[r]) return;
+  const RveDesc d = a.desc[r];
+  const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+  const int64_t G = 8 * E;
+  const double jw = d.hx * d.hy * d.hz / 8.0;
+  const double dt = a.dt[r];
+  double S[RVE_NSUM];
+#pragma unroll
+  for (int t = 0; t < RVE_NSUM; ++t) S[t] = 0.0;
+  double mmin = INFINITY, mmax = -INFINITY, qmax[RVE_MAX_PHASES];
+#pragma unroll
+  for (int t = 0; t < RVE_MAX_PHASES; ++t) qmax[t] = -INFINITY;
+  const int64_t rounds = (G + blockDim.x - 1) / blockDim.x;
+  for (int64_t it = 0; it < rounds; ++it) {
+    const int64_t gl = it * blockDim.x + threadIdx.x;
+    const bool live = gl < G;
+    const int64_t le = live ? (gl >> 3) : 0;
+    const int q = (int)(gl & 7);
+    int i, j, k;
+    local_ijk(d, le, i, j, k);
+    const int64_t e = d.eoff + le;
+    const int64_t g = 8 * e + q;
+    double w1[3] = {0, 0, 0}, w0[3] = {0, 0, 0};
+    if (live) {
+      const int64_t node = element_node(d, i, j, k, q);
+      load_w(a.w, nullptr, 0.0, node, w1);
+      load_w(a.w_n, nullptr, 0.0, node, w0);
+    }
+    double u1[8][3], u0[8][3];
+    allgather8(w1, u1);
+    allgather8(w0, u0);
+    Grad8<double> Gr;
+    physical_grads(q, d, Gr);
+    double eps[6], eps0[6];
+    strain_from(Gr, u1, eps);
+    strain_from(Gr, u0, eps0);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      eps[c] += a.macro[6 * r + c];
+      eps0[c] += a.macro_n[6 * r + c];
+    }
+    if (!live) continue;
+    const int ph = (int)a.phase[e];
+    const PhaseMat<double>& m = a.mats.m[ph];
+    double sig[6], de[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      sig[c] = (double)a.stress[c * a.ngp + g];
+      de[c] = eps[c] - eps0[c];
+    }
+    // Per-point energy, dissipation and increment diagnostics.
+    double psi, diss = 0.0, iwd, esi, margin = NAN, active = 0.0;
+    double sprev[6];
+    if (m.kind == PHASE_J2VP) {
+      // Re-run the return map of this update in the kernel precision (same inputs and
+      // operation order as the residual pass) for the local-solver diagnostics.
+      const PhaseMat<T>& mt = a.mats_t.m[ph];
+      T wt[3] = {(T)w1[0], (T)w1[1], (T)w1[2]};
+      T ut[8][3];
+      // all lanes of this group are live here; the group never straddles the G boundary
+      {
+        const int base = (threadIdx.x & 31) & ~7;
+        const unsigned gmask = 0xffu << base;
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+#pragma unroll
+          for (int dd = 0; dd < 3; ++dd) ut[b][dd] = __shfl_sync(gmask, wt[dd], base + b);
+      }
+      Grad8<T> Gt;
+      physical_grads(q, d, Gt);
+      T et[6], ep0t[6], eelt[6], stt[6];
+      strain_from(Gt, ut, et);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        et[c] += (T)a.macro[6 * r + c];
+        ep0t[c] = a.ep_n[c * a.ngp + g];
+        eelt[c] = et[c] - ep0t[c];
+      }
+      elastic_stress(mt.j2, eelt, stt);
+      const double q0 = a.q_n[g];
+      J2Out<T> o;
+      const int st_code = j2vp_point<T, false>(mt.j2, (T)dt, stt, q0, o);
+      const bool act = (st_code == CIB_J2_OK) && o.active;
+      double ep1[6], ep0[6], ee[6], se[6], e_prev[6];
+      const double q1 = a.q[g];
+      const double dg = q1 - q0;
+      double pw = 0.0, wsum = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        ep1[c] = (double)a.ep[c * a.ngp + g];
+        ep0[c] = (double)a.ep_n[c * a.ngp + g];
+        ee[c] = eps[c] - ep1[c];
+        pw += sig[c] * (ep1[c] - ep0[c]);
+        e_prev[c] = (eps[c] - de[c]) - ep0[c];
+      }
+      elastic_stress(m.j2, ee, se);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) wsum += se[c] * ee[c];
+      psi = 0.5 * wsum + 0.5 * m.j2.H * q1 * q1;
+      active = act ? 1.0 : 0.0;
+      if (act) diss = pw / dt - m.j2.H * q1 * dg / dt;
+      elastic_stress(m.j2, e_prev, sprev);
+      const double ftr = (double)o.f_tr, ys = (double)o.yield_scale, thr = (double)o.threshold;
+      margin = (ftr - thr) / ys;
+      if (a.diag) {
+        const int64_t Gt_ = a.ngp;
+        double* dgr = a.diag;
+        double dv2[6];
+        const double qf = act ? sqrt(fmax(j2_radicand(sig, dv2), 0.0)) : (double)o.q_tr;
+        const double fy = act ? qf - (m.j2.sy + m.j2.H * q1) : ftr;
+        dgr[0 * Gt_ + g] = fy;
+        dgr[1 * Gt_ + g] = act ? pw : 0.0;
+        dgr[2 * Gt_ + g] = (double)o.iters;
+        dgr[3 * Gt_ + g] = act ? 4.0 : 0.0;
+        dgr[4 * Gt_ + g] = dg;
+        dgr[5 * Gt_ + g] = dg;
+        dgr[6 * Gt_ + g] = qf;
+        dgr[7 * Gt_ + g] = ftr;
+        dgr[8 * Gt_ + g] = ys;
+        dgr[9 * Gt_ + g] = thr;
+        dgr[10 * Gt_ + g] = margin;
+        dgr[11 * Gt_ + g] = active;
+        dgr[12 * Gt_ + g] = dt;
+        dgr[13 * Gt_ + g] = q1;
+        dgr[14 * Gt_ + g] = act ? (double)o.hv : 0.0;
+        dgr[15 * Gt_ + g] = act ? pw / dt : 0.0;
+        dgr[16 * Gt_ + g] = act ? m.j2.H * q1 * dg / dt : 0.0;
+        dgr[17 * Gt_ + g] = act ? (double)o.local_residual : 0.0;
+        dgr[18 * Gt_ + g] = 0.0;
+        dgr[19 * Gt_ + g] = act ? ftr / m.j2.slope : 0.0;
+      }
+    } else {
+      double w_ = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) w_ += eps[c] * sig[c];
+      psi = 0.5 * w_;
+      double ds[6];
+      elastic_stress(m.j2, de, ds);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) sprev[c] = sig[c] - ds[c];
+    }
+    {
+      double w_ = 0.0, dv[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) w_ += (sprev[c] + sig[c]) * de[c];
+      iwd = 0.5 * w_;
+      esi = sqrt(fmax(j2_radicand(sig, dv), 0.0)) - sqrt(fmax(j2_radicand(sprev, dv), 0.0));
+    }
+    if (a.diag) {
+      a.diag[20 * a.ngp + g] = iwd;
+      a.diag[21 * a.ngp + g] = esi;
+      if (m.kind != PHASE_J2VP) {
+        // elastic phase: only the phased-model rows exist (others are NaN in the reference)
+        for (int row = 0; row < 20; ++row) a.diag[row * a.ngp + g] = NAN;
+        a.diag[11 * a.ngp + g] = 0.0;
+      }
+    }
+    if (a.point_out) {
+      // strains, strain rates, free energy, dissipation
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        a.point_out[c * a.ngp + g] = eps[c];
+        a.point_out[(6 + c) * a.ngp + g] = de[c] / dt;
+      }
+      a.point_out[12 * a.ngp + g] = psi;
+      a.point_out[13 * a.ngp + g] = diss;
+    }
+    double mw = 0.0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      S[RS_SIGMA + c] += sig[c] * jw;
+      mw += sig[c] * de[c];
+    }
+    S[RS_PSI] += psi * jw;
+    S[RS_DISS] += diss * jw;
+    S[RS_MICRO_WORK] += mw * jw;
+    S[RS_POS_WORK] += fmax(iwd, 0.0) * jw;
+    S[RS_NEG_WORK] += fmin(iwd, 0.0) * jw;
+    if (iwd < 0.0) S[RS_UNLOAD] += jw;
+    if (active > 0.5) S[RS_ACTIVE] += jw;
+    if (m.kind == PHASE_J2VP) {
+      S[RS_EQPS] += a.q[g] * jw;
+      if (isfinite(margin)) {
+        mmin = fmin(mmin, margin);
+        mmax = fmax(mmax, margin);
+      }
+    }
+    if (ph < RVE_MAX_PHASES) {
+      double* P = S + RS_PHASE + ph * RS_PHASE_STRIDE;
+      P[0] += jw;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) P[1 + c] += sig[c] * jw;
+      P[7] += psi * jw;
+      P[8] += diss * jw;
+      if (m.kind == PHASE_J2VP) {
+        P[9] += a.q[g] * jw;
+        qmax[ph] = fmax(qmax[ph], a.q[g]);
+      }
+    }
+  }
+  // Virtual-work stress A^T f / V, full nodal force norm and face resultants from the
+  // element nodal forces of the last residual pass (physical, non-periodic nodes).
+  const int64_t NX = d.nx + 1, NY = d.ny + 1, NZ = d.nz + 1;
+  const int64_t NN = NX * NY * NZ;
+  for (int64_t n = threadIdx.x; n < NN; n += blockDim.x) {
+    const int I = (int)(n % NX), J = (int)((n / NX) % NY), K = (int)(n / (NX * NY));
+    double f[3] = {0, 0, 0};
+    for (int s = 0; s < 8; ++s) {
+      const int di = s & 1, dj = (s >> 1) & 1, dk = (s >> 2) & 1;
+      const int ie = I - di, je = J - dj, ke = K - dk;
+      if (ie < 0 || je < 0 || ke < 0 || ie >= d.nx || je >= d.ny || ke >= d.nz) continue;
+      const int64_t e = d.eoff + ie + (int64_t)d.nx * (je + (int64_t)d.ny * ke);
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) f[dd] += a.fe[(8 * e + s) * 3 + dd];
+    }
+    const double x = I * d.hx, y = J * d.hy, z = K * d.hz;
+    S[RS_VW + 0] += x * f[0];
+    S[RS_VW + 1] += y * f[1];
+    S[RS_VW + 2] += z * f[2];
+    S[RS_VW + 3] += 0.5 * (z * f[1] + y * f[2]);
+    S[RS_VW + 4] += 0.5 * (z * f[0] + x * f[2]);
+    S[RS_VW + 5] += 0.5 * (y * f[0] + x * f[1]);
+    S[RS_FNORM2] += f[0] * f[0] + f[1] * f[1] + f[2] * f[2];
+    const int idx[3] = {I, J, K};
+    const int64_t mx[3] = {d.nx, d.ny, d.nz};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      if (idx[ax] == 0)
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) S[RS_FACE + 6 * ax + dd] += f[dd];
+      if (idx[ax] == mx[ax])
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) S[RS_FACE + 6 * ax + 3 + dd] += f[dd];
+    }
+    // periodic fluctuation mismatch of u = T w + A ebar against the class representative
+    double w[3];
+    load_w(a.w, nullptr, 0.0, periodic_node(d, I, J, K), w);
+    const double* eb = a.macro + 6 * r;
+    const double ua[3] = {x * eb[0] + 0.5 * z * eb[4] + 0.5 * y * eb[5], y * eb[1] + 0.5 * z * eb[3] + 0.5 * x * eb[5],
+                          z * eb[2] + 0.5 * y * eb[3] + 0.5 * x * eb[4]};
+    const double xr = (I % d.nx) * d.hx, yr = (J % d.ny) * d.hy, zr = (K % d.nz) * d.hz;
+    const double ur[3] = {xr * eb[0] + 0.5 * zr * eb[4] + 0.5 * yr * eb[5],
+                          yr * eb[1] + 0.5 * zr * eb[3] + 0.5 * xr * eb[5],
+                          zr * eb[2] + 0.5 * yr * eb[3] + 0.5 * xr * eb[4]};
+    double mis = 0.0;
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      const double fl = (w[dd] + ua[dd]) - ua[dd];
+      const double flr = (w[dd] + ur[dd]) - ur[dd];
+      mis += (fl - flr) * (fl - flr);
+    }
+    S[RS_PERIODIC] = fmax(S[RS_PERIODIC], sqrt(mis));
+  }
+  const double pmax = block_max(S[RS_PERIODIC], scratch);
+  S[RS_PERIODIC] = 0.0;
+  mmin = block_min(mmin, scratch);
+  mmax = block_max(mmax, scratch);
+  for (int t = 0; t < RVE_MAX_PHASES; ++t) qmax[t] = block_max(qmax[t], scratch);
+  block_sum<RVE_NSUM>(S, scratch);
+  if (threadIdx.x == 0) {
+    double* o = a.sums + (int64_t)r * RVE_NOUT;
+    for (int t = 0; t < RVE_NSUM; ++t) o[t] = S[t];
+    o[RS_PERIODIC] = pmax;
+    o[RVE_NSUM + 0] = mmin;
+    o[RVE_NSUM + 1] = mmax;
+    for (int t = 0; t < RVE_MAX_PHASES; ++t) o[RVE_NSUM + 2 + t] = qmax[t];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Host launchers.
+
+template <typename T>
+int launch_rve_residual(const RveResidualArgs<T>& a, int nrve, cudaStream_t st) {
+  rve_residual_kernel<T><<<nrve, RVE_THREADS, 0, st>>>(a);
+  return check_launch();
+}
+
+int launch_rve_gather(const RveGatherArgs& a, int nrve, cudaStream_t st) {
+  rve_gather_kernel<<<nrve, RVE_THREADS, 0, st>>>(a);
+  return check_launch();
+}
+
+template <typename T>
+int launch_rve_pcg(const RvePcgArgs<T>& a, int nsys, int max_nxy, cudaStream_t st) {
+  const size_t smem = (size_t)max_nxy * (24 + 9) * sizeof(double);
+  if (smem > 200 * 1024) return CIB_ERANGE;
+  static bool configured[2] = {false, false};
+  const int slot = sizeof(T) == 8 ? 1 : 0;
+  if (!configured[slot]) {
+    if (cudaFuncSetAttribute(rve_pcg_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+        cudaSuccess)
+      return check_launch();
+    configured[slot] = true;
+  }
+  rve_pcg_kernel<T><<<nsys, RVE_THREADS, smem, st>>>(a);
+  return check_launch();
+}
+
+template <typename T>
+int launch_rve_tangent_rhs(const RveTangentArgs<T>& a, int nrve, cudaStream_t st) {
+  rve_tangent_rhs_kernel<T><<<nrve, RVE_THREADS, 0, st>>>(a);
+  return check_launch();
+}
+
+int launch_rve_tangent_finish(const RveTangentFinishArgs& a, int nrve, cudaStream_t st) {
+  rve_tangent_finish_kernel<<<nrve, RVE_THREADS, 0, st>>>(a);
+  return check_launch();
+}
+
+template <typename T>
+int launch_rve_response(const RveResponseArgs<T>& a, int nrve, cudaStream_t st) {
+  rve_response_kernel<T><<<nrve, RVE_THREADS, 0, st>>>(a);
+  return check_launch();
+}
+
+template int launch_rve_residual<float>(const RveResidualArgs<float>&, int, cudaStream_t);
+template int launch_rve_residual<double>(const RveResidualArgs<double>&, int, cudaStream_t);
+template int launch_rve_pcg<float>(const RvePcgArgs<float>&, int, int, cudaStream_t);
+template int launch_rve_pcg<double>(const RvePcgArgs<double>&, int, int, cudaStream_t);
+template int launch_rve_tangent_rhs<float>(const RveTangentArgs<float>&, int, cudaStream_t);
+template int launch_rve_tangent_rhs<double>(const RveTangentArgs<double>&, int, cudaStream_t);
+template int launch_rve_response<float>(const RveResponseArgs<float>&, int, cudaStream_t);
+template int launch_rve_response<double>(const RveResponseArgs<double>&, int, cudaStream_t);
+
+}  // namespace cib

@@ -1,0 +1,231 @@
+"""Builders and drivers around the periodic RVE solve.
+
+* ``sphere_phase_map`` / ``build_two_phase_sphere_rve`` -- two-phase concrete RVE on a
+  structured box: an element belongs to the aggregate phase when its centroid lies in one
+  of a set of non-overlapping, periodically wrapped spheres with radii U[r_min, r_max],
+  drawn by seeded rejection until the spheres' volume reaches the target fraction.  The
+  reference builds its two-phase RVEs from a cylindrical O-grid
+  (src/fem/rve/builders.py:22-78); this box builder keeps its PhasedMaterialModel layout
+  (phase names, point_phase_ids, effective density; src/fem/materials/phased.py:36-66).
+* ``build_structured_rve`` -- single-material structured RVE as in the reference's tests
+  (tests/unit/fem/test_rve.py:223-246).
+* ``solve_mixed_control_step`` -- one macro step where some macro strain components are
+  prescribed and the others are free (their macro stress vanishes), solved by an outer
+  Newton on the RVE's effective tangent around solve_rve_microequilibrium.
+* ``random_strain_path`` -- piecewise-linear 6-component macro strain path with a
+  prescribed strain rate, for batched path generation.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Any, Callable
+
+import numpy as np
+
+from .materials import MaterialResponseRequirements, PhasedMaterialModel, RVEPhase
+from .rve import (
+    NonlinearNewtonSettings,
+    RVERequest,
+    RVEResponse,
+    RVEState,
+    StructuredHex8RVE,
+    build_structured_hex8_box,
+    build_structured_hex8_periodic_constraint,
+)
+
+
+@dataclass(frozen=True)
+class SphereLayout:
+    """Spheres (centres, radii) of a periodic unit-cell inclusion layout."""
+
+    centres: np.ndarray
+    radii: np.ndarray
+    target_fraction: float
+    sphere_fraction: float
+
+
+def draw_spheres(seed: int, target_fraction: float = 0.4, r_min: float = 0.08, r_max: float = 0.15,
+                 lengths=(1.0, 1.0, 1.0), max_attempts: int = 200_000, batch: int = 512) -> SphereLayout:  # fmt: skip
+    """Seeded random sequential addition of non-overlapping periodic spheres.
+
+    Candidates (radius, centre) are drawn in batches; each is tested, in draw order,
+    against every sphere accepted before it (minimum-image distance), so the result is
+    that of one-at-a-time rejection sampling of the same random stream."""
+    rng = np.random.default_rng(seed)
+    box = np.asarray(lengths, dtype=np.float64)
+    volume = float(np.prod(box))
+    centres = np.zeros((0, 3))
+    radii = np.zeros(0)
+    filled = 0.0
+    drawn = 0
+    while drawn < max_attempts and filled < target_fraction * volume:
+        m = min(batch, max_attempts - drawn)
+        r = rng.uniform(r_min, r_max, size=m)
+        c = rng.uniform(0.0, 1.0, size=(m, 3)) * box
+        drawn += m
+        if radii.size:
+            d = c[:, None, :] - centres[None, :, :]
+            d -= box * np.round(d / box)
+            clash = np.any(np.linalg.norm(d, axis=2) < r[:, None] + radii[None, :], axis=1)
+        else:
+            clash = np.zeros(m, dtype=bool)
+        for t in np.flatnonzero(~clash):
+            if filled >= target_fraction * volume:
+                break
+            if radii.size:
+                dd = centres - c[t]
+                dd -= box * np.round(dd / box)
+                if np.any(np.linalg.norm(dd, axis=1) < radii + r[t]):
+                    continue
+            centres = np.vstack([centres, c[t]])
+            radii = np.append(radii, r[t])
+            filled += 4.0 / 3.0 * np.pi * r[t] ** 3
+    return SphereLayout(centres, radii, target_fraction, filled / volume)
+
+
+def sphere_phase_map(divisions, layout: SphereLayout, lengths=(1.0, 1.0, 1.0)) -> np.ndarray:
+    """Element phase ids: 1 (aggregate) where the element centroid lies in a sphere, else 0."""
+    nx, ny, nz = divisions
+    box = np.asarray(lengths, dtype=np.float64)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    centroids = np.column_stack([(i.ravel() + 0.5) * box[0] / nx, (j.ravel() + 0.5) * box[1] / ny,
+                                 (k.ravel() + 0.5) * box[2] / nz])  # fmt: skip
+    inside = np.zeros(centroids.shape[0], dtype=bool)
+    for c, r in zip(layout.centres, layout.radii):
+        d = centroids - c
+        d -= box * np.round(d / box)
+        inside |= np.einsum("ij,ij->i", d, d) <= r * r
+    return inside.astype(np.int64)
+
+
+def build_structured_rve(divisions, material, newton_settings: NonlinearNewtonSettings, lengths=(1.0, 1.0, 1.0),
+                         hill_mandel_power_scale: float = 1.0) -> StructuredHex8RVE:  # fmt: skip
+    """Single-material structured periodic RVE."""
+    nodes, elements = build_structured_hex8_box(tuple(lengths), tuple(divisions))
+    constraint = build_structured_hex8_periodic_constraint(nodes, tuple(divisions))
+    return StructuredHex8RVE(nodes, elements, tuple(divisions), material, constraint, newton_settings,
+                             hill_mandel_power_scale=hill_mandel_power_scale)  # fmt: skip
+
+
+def build_two_phase_sphere_rve(divisions, matrix_material, inclusion_material, newton_settings: NonlinearNewtonSettings,
+                               seed: int, target_fraction: float = 0.4, r_min: float = 0.08, r_max: float = 0.15,
+                               lengths=(1.0, 1.0, 1.0), hill_mandel_power_scale: float = 1.0,
+                               phase_names=("matrix", "inclusion")) -> StructuredHex8RVE:  # fmt: skip
+    """Two-phase periodic box RVE: phase 0 matrix (mortar), phase 1 inclusion (aggregate)."""
+    nodes, elements = build_structured_hex8_box(tuple(lengths), tuple(divisions))
+    layout = draw_spheres(seed, target_fraction, r_min, r_max, lengths)
+    element_phase = sphere_phase_map(divisions, layout, lengths)
+    n_el = elements.shape[0]
+    frac = element_phase.mean() if n_el else 0.0
+    density = matrix_material.density * (1.0 - frac) + inclusion_material.density * frac
+    phased = PhasedMaterialModel(
+        name=f"{matrix_material.name}__{inclusion_material.name}",
+        phases=(RVEPhase(phase_names[0], matrix_material), RVEPhase(phase_names[1], inclusion_material)),
+        point_phase_ids=np.repeat(element_phase, 8),
+        effective_density=float(density),
+    )
+    constraint = build_structured_hex8_periodic_constraint(nodes, tuple(divisions))
+    return StructuredHex8RVE(
+        nodes, elements, tuple(divisions), phased, constraint, newton_settings,
+        element_phase_ids=element_phase,
+        element_densities=np.where(element_phase == 0, matrix_material.density, inclusion_material.density),
+        phase_names=tuple(phase_names), hill_mandel_power_scale=hill_mandel_power_scale,
+    )  # fmt: skip
+
+
+@dataclass(frozen=True)
+class MixedControlResult:
+    """Outcome of one mixed strain/stress controlled macro step."""
+
+    response: RVEResponse
+    macro_strain: np.ndarray
+    outer_iterations: int
+    free_stress_norm: float
+
+
+def solve_mixed_control_step(
+    solve: Callable[[RVERequest, RVEState], RVEResponse],
+    state: RVEState,
+    prescribed: dict[int, float],
+    guess: np.ndarray,
+    time_step: float,
+    update_settings,
+    stress_tolerance: float,
+    max_outer: int = 20,
+) -> MixedControlResult:
+    """Find the free macro strain components so that their macro stress vanishes.
+
+    ``solve(request, state)`` is one RVE microequilibrium solve from the committed state
+    (e.g. solve_rve_microequilibrium with a bound model and cache).  Each outer iteration
+    corrects the free components with the effective tangent's free-free block.
+    """
+    strain = np.asarray(guess, dtype=np.float64).copy()
+    for comp, value in prescribed.items():
+        strain[comp] = value
+    free = [c for c in range(6) if c not in prescribed]
+    response = None
+    norm = np.inf
+    for outer in range(1, max_outer + 1):
+        response = solve(RVERequest(strain.copy(), time_step, update_settings,
+                                    MaterialResponseRequirements(tangent=True)), state)  # fmt: skip
+        stress = np.asarray(response.macro_stress, dtype=np.float64)
+        norm = float(np.linalg.norm(stress[free]))
+        if norm <= stress_tolerance:
+            return MixedControlResult(response, strain, outer, norm)
+        tangent = np.asarray(response.effective_tangent, dtype=np.float64)
+        strain[free] -= np.linalg.solve(tangent[np.ix_(free, free)], stress[free])
+    raise RuntimeError(f"mixed control did not converge: free stress norm {norm:.3e} after {max_outer} iterations")
+
+
+def random_strain_path(seed: int, steps: int = 200, segments: int = 4, max_abs: float = 1.0e-2,
+                       rate_range=(1.0, 1000.0)) -> tuple[np.ndarray, np.ndarray]:  # fmt: skip
+    """Piecewise-linear macro strain path: ``segments`` vertices uniform in the ball of
+    radius ``max_abs`` (6 components, then clipped to |strain| <= max_abs), strain rate
+    log-uniform in ``rate_range`` (1/s); returns (times (steps+1,), strains (steps+1, 6))."""
+    rng = np.random.default_rng(seed)
+    vertices = [np.zeros(6)]
+    for _ in range(segments):
+        v = rng.standard_normal(6)
+        v *= rng.uniform(0.0, 1.0) ** (1.0 / 6.0) * max_abs / np.linalg.norm(v)
+        vertices.append(np.clip(v, -max_abs, max_abs))
+    vertices = np.asarray(vertices)
+    seg_len = np.linalg.norm(np.diff(vertices, axis=0), axis=1)
+    arc = np.concatenate([[0.0], np.cumsum(seg_len)])
+    s = np.linspace(0.0, arc[-1], steps + 1)
+    strains = np.column_stack([np.interp(s, arc, vertices[:, c]) for c in range(6)])
+    rate = float(np.exp(rng.uniform(np.log(rate_range[0]), np.log(rate_range[1]))))
+    times = s / rate
+    if times[-1] == 0.0:
+        times = np.arange(steps + 1, dtype=np.float64) * 1e-6
+    return times, strains
+
+
+def config0_materials():
+    """Mortar (J2 Perzyna) and aggregate (linear elastic) of the concrete RVE, SI units."""
+    from .materials import J2ViscoplasticMaterial, LinearElasticMaterial
+
+    mortar = J2ViscoplasticMaterial("mortar", 2200.0, 25.0e9, 0.2, 20.0e6, 2.0e9, 1.0e-3, 20.0e6, 1.0)
+    aggregate = LinearElasticMaterial("aggregate", 2600.0, 50.0e9, 0.2)
+    return mortar, aggregate
+
+
+def default_newton(armijo: bool = False) -> NonlinearNewtonSettings:
+    """Newton settings of the concrete RVE runs (relative residual tolerance 1e-8)."""
+    from .rve import ArmijoSettings
+
+    return NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=armijo))
+
+
+def uniaxial_path(steps: int = 100, final_strain: float = -5.0e-3, rate: float = 10.0) -> tuple[np.ndarray, np.ndarray]:
+    """Times and prescribed xx strain of the uniaxial compression ramp."""
+    exx = np.linspace(0.0, final_strain, steps + 1)
+    times = np.abs(exx) / rate
+    return times, exx
+
+
+def describe(model: StructuredHex8RVE) -> dict[str, Any]:
+    """Small summary of a two-phase RVE (phase fractions, sizes)."""
+    phase = model.element_phase_ids
+    return {"divisions": model.divisions, "elements": int(model.elements.shape[0]),
+            "inclusion_fraction": float(np.mean(phase)) if phase is not None else 0.0}  # fmt: skip

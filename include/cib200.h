@@ -173,6 +173,103 @@ int cib_linear_elastic_update(double young_modulus, double poisson_ratio, int64_
                               double* tangent, double* free_energy, double* dissipation,
                               double* increment_diagnostics, void* stream);
 
+/* --- Periodic structured Hex8 RVE batch ------------------------------------------------
+ * A batch holds R structured periodic RVEs (unit-cell boxes of nx*ny*nz Hex8 elements).
+ * RVE r owns elements [elem_offset, elem_offset + nx*ny*nz); its periodic node (class)
+ * c = i + nx*(j + ny*k) is batch node elem_offset + c; class 0 is the eliminated
+ * reference class (src/fem/rve/periodic.py:20-104).  Periodic vectors (fluctuation w,
+ * residual, PCG vectors) are float64 with 3 entries per batch node.  Gauss-point arrays
+ * are SoA over the 8*nelem points (point 8*e + q).  The element arithmetic type is
+ * float64 or float32 (`precision`); equivalent plastic strain and the viscoplastic
+ * multiplier are always float64.  All arrays are device memory except `mats`. */
+#define CIB_RVE_MAX_PHASES 8
+#define CIB_RVE_NOUT 130
+#define CIB_PHASE_LINEAR_ELASTIC 0
+#define CIB_PHASE_J2_VISCOPLASTIC 1
+
+typedef struct cib_rve_desc {
+  int32_t nx, ny, nz, pad_;
+  int64_t elem_offset;
+  double hx, hy, hz; /* element edge lengths */
+} cib_rve_desc;
+
+typedef struct cib_phase_material {
+  int32_t kind; /* CIB_PHASE_* */
+  int32_t pad_;
+  cib_j2vp_material params; /* young_modulus / poisson_ratio used by both kinds */
+} cib_phase_material;
+
+typedef struct cib_rve_batch {
+  int32_t nrve;
+  int32_t nphase;
+  int64_t nelem;             /* total elements = total periodic nodes */
+  int32_t precision;         /* 64 or 32 */
+  int32_t max_nxy;           /* max nx*ny over the batch (PCG shared memory) */
+  const cib_rve_desc* desc;  /* device, nrve */
+  const uint8_t* phase;      /* device, nelem: phase id per element */
+  cib_phase_material mats[CIB_RVE_MAX_PHASES];
+  cib_update_settings settings;
+  /* committed Gauss-point state */
+  const void* plastic_strain_n; /* T, 6 x 8*nelem */
+  const double* eqps_n;         /* 8*nelem */
+  const double* vpm_n;          /* 8*nelem */
+  /* trial Gauss-point state and tangent data (written by cib_rve_residual) */
+  void* plastic_strain;         /* T, 6 x 8*nelem */
+  double* eqps;
+  double* vpm;
+  void* stress;                 /* T, 6 x 8*nelem */
+  void* tparam;                 /* T, 8 x 8*nelem: flow direction (6), f, c */
+  uint8_t* tflag;               /* 8*nelem: 1 where the consistent tangent is viscoplastic */
+  /* element work arrays (caller-provided scratch) */
+  double* fe;                   /* 24 * nelem: element nodal forces */
+  double* de;                   /* 24 * nelem: element tangent diagonals */
+} cib_rve_batch;
+
+/* Fused residual pass (nonlinear_solid.py:428-493 + solver.py:88-100): for every Gauss
+ * point, strain = macro + B (w + alpha dw) on the periodic mesh, return map from the
+ * committed state, trial state, stress, tangent data, element nodal forces w B^T sigma and
+ * element tangent diagonals.  time_step and macro: 1 and 6 per RVE; dw and alpha (per RVE) may be NULL;
+ * inactive RVEs (active[r] == 0) are skipped.  fail: one word per RVE, lowest failing
+ * local point index (initialised to CIB_NO_FAILURE by the caller). */
+int cib_rve_residual(const cib_rve_batch* batch, const double* time_step, const double* macro, const double* w,
+                     const double* dw, const double* alpha, const int32_t* active, unsigned long long* fail,
+                     void* stream);
+
+/* Periodic gather of the last residual pass: reduced residual r = T^T f_int (class 0
+ * removed, solver.py:97-100), inverse Jacobi diagonal, ||r||^2, ||w + alpha dw||^2 and the
+ * largest class force (class 0 included) per RVE; optional w_out = w + alpha dw. */
+int cib_rve_gather(const cib_rve_batch* batch, const double* w, const double* dw, const double* alpha,
+                   const int32_t* active, double* residual, double* dinv, double* rnorm2, double* wnorm2,
+                   double* class_max, double* w_out, void* stream);
+
+/* Jacobi-preconditioned CG on the reduced periodic tangent of the last residual pass
+ * (replaces the reference's Tt K T + spsolve, solver.py:143-144), one system per CTA:
+ * system s belongs to RVE sys_rve[s] and its vectors start at sys_off[s] (doubles) in b,
+ * x, r, p and Ap.  Stops when ||r|| <= rtol ||b|| or after maxit iterations; status 0
+ * converged, 1 iteration limit, 2 breakdown. */
+int cib_rve_pcg(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve, const int64_t* sys_off,
+                const int32_t* active, const double* b, const double* dinv, double* x, double* r, double* p,
+                double* Ap, double rtol, int32_t maxit, int32_t* status, int32_t* iterations,
+                double* rel_residual, double* xnorm, void* stream);
+
+/* Effective tangent (solver.py:438-461): right-hand sides K_we = T^T K A (6 columns per
+ * RVE, layout [18*elem_offset + j*3*E_r + 3*c + d]) and K_ee = A^T K A (36 per RVE);
+ * fe6 is scratch of 6*24*nelem doubles.  Then C = (K_ee - K_we^T S) / V from the PCG
+ * solutions S (same layout). */
+int cib_rve_tangent_rhs(const cib_rve_batch* batch, const int32_t* active, double* fe6, double* rhs, double* kee,
+                        void* stream);
+int cib_rve_tangent_finish(const cib_rve_batch* batch, const int32_t* active, const double* rhs, const double* sol,
+                           const double* kee, double* ceff, void* stream);
+
+/* Homogenisation and diagnostics of a converged state (solver.py:253-364, 464-494):
+ * CIB_RVE_NOUT doubles per RVE (sums of stress, energy, work, activity and phase
+ * quantities, virtual-work and reaction sums, periodicity mismatch, activation-margin
+ * extrema); optional per-point outputs: point_out (14 x 8*nelem: strain 6, strain rate 6,
+ * free energy, dissipation) and diagnostics (CIB_J2_NDIAG x 8*nelem). */
+int cib_rve_response(const cib_rve_batch* batch, const double* time_step, const double* macro, const double* macro_n,
+                     const double* w, const double* w_n, const int32_t* active, double* sums, double* point_out,
+                     double* diagnostics, void* stream);
+
 /* Strided host<->device copy of `rows` rows of `row_bytes` bytes (one cudaMemcpy2DAsync);
  * kind 1 = host to device, 2 = device to host, 3 = device to device. */
 int cib_copy_rows_async(void* dst, int64_t dst_pitch, const void* src, int64_t src_pitch, int64_t row_bytes,

@@ -160,6 +160,97 @@ def make_failure_cases(data_mod, plasticity, errors):
     return out
 
 
+def _rve_arrays(prefix: str, response, macro) -> dict:
+    out = {f"{prefix}macro_strain": macro, f"{prefix}macro_stress": response.macro_stress,
+           f"{prefix}fluctuation": response.state.fluctuation_dofs,
+           f"{prefix}micro_stresses": response.micro_stresses,
+           f"{prefix}micro_strains": response.micro_strains}  # fmt: skip
+    if response.effective_tangent is not None:
+        out[f"{prefix}effective_tangent"] = response.effective_tangent
+    for name, values in response.state.material_state.variables.items():
+        out[f"{prefix}state__{name}"] = values
+    for name, values in response.micro_diagnostics.items():
+        out[f"{prefix}mdiag__{name}"] = values
+    scalars = {k: v for k, v in response.diagnostics.items() if isinstance(v, (int, float))}
+    scalars["free_energy_density"] = response.free_energy_density
+    scalars["dissipation_density"] = response.dissipation_density
+    return out, scalars
+
+
+def make_rve_cases():
+    """RVE solves of the reference on structured periodic boxes (homogeneous and two-phase)."""
+    from fem.materials.data import MaterialResponseRequirements
+    from fem.materials.linear_elastic import LinearElasticMaterial
+    from fem.materials.phased import PhasedMaterialModel, RVEPhase
+    from fem.materials.plasticity import J2ViscoplasticMaterial
+    from fem.mesh.structured import build_structured_hex8_box
+    from fem.rve import (RVERequest, StructuredHex8RVE, build_structured_hex8_periodic_constraint,
+                         initialize_rve_state, solve_rve_microequilibrium)  # fmt: skip
+    from fem.solvers.data import ArmijoSettings, NonlinearNewtonSettings
+    from fem.materials.data import MaterialUpdateSettings
+
+    sys.path.insert(0, str(REPO))
+    from concrete_impact_b200.rve_builders import draw_spheres, sphere_phase_map
+
+    cases = {}
+    update = MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10)
+    # (1) homogeneous RVE of the reference unit test (m = 2, Armijo), 4-step path
+    mat = J2ViscoplasticMaterial("single_phase_rve_j2", 1.0, 3339.9160679991464, 0.36994096308414537, 10.0, 80.0,
+                                 0.02, 10.0, 2.0)  # fmt: skip
+    path = [np.asarray([0.002, -0.0005, -0.0005, 0.0, 0.0, 0.01]),
+            np.asarray([0.004, -0.0010, -0.0010, 0.002, -0.003, 0.02]),
+            np.asarray([0.003, -0.0008, -0.0008, 0.001, -0.002, 0.012]),
+            np.asarray([0.0045, -0.0012, -0.0012, -0.001, 0.002, -0.01])]  # fmt: skip
+    newton_h = NonlinearNewtonSettings(20, 1.0e-10, 1.0e-10, 1.0e-12, 1.0e-10, ArmijoSettings(enabled=True))
+    for div in ((1, 1, 1), (2, 2, 2)):
+        nodes, elements = build_structured_hex8_box((1.0, 1.0, 1.0), div)
+        model = StructuredHex8RVE(nodes, elements, div, mat, build_structured_hex8_periodic_constraint(nodes, div),
+                                  newton_h, hill_mandel_power_scale=10.0)  # fmt: skip
+        state = initialize_rve_state(model)
+        arrays, meta_steps = {}, []
+        for step, macro in enumerate(path):
+            response = solve_rve_microequilibrium(model, RVERequest(macro, 1.0e-3, update), state)
+            a, sc = _rve_arrays(f"s{step}__", response, macro)
+            arrays.update(a)
+            meta_steps.append(sc)
+            state = response.state
+        meta = {"kind": "homogeneous", "divisions": div, "time_step": 1.0e-3, "steps": len(path), "scalars": meta_steps,
+                "material": {"params": dict(young_modulus=mat.young_modulus, poisson_ratio=mat.poisson_ratio,
+                             yield_stress=mat.yield_stress, hardening_modulus=mat.hardening_modulus,
+                             time_scale=mat.time_scale, reference_stress=mat.reference_stress,
+                             rate_exponent=mat.rate_exponent)},
+                "newton": [20, 1.0e-10, 1.0e-10, 1.0e-12, 1.0e-10, True], "hill_mandel_power_scale": 10.0}  # fmt: skip
+        cases[f"rve_homogeneous_{div[0]}"] = (arrays, meta)
+    # (2) two-phase concrete RVEs: mortar J2 Perzyna + elastic aggregate, sphere layouts
+    mortar = J2ViscoplasticMaterial("mortar", 2200.0, 25.0e9, 0.2, 20.0e6, 2.0e9, 1.0e-3, 20.0e6, 1.0)
+    aggregate = LinearElasticMaterial("aggregate", 2600.0, 50.0e9, 0.2)
+    newton_c = NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=False))
+    direction = np.asarray([-1.0, 0.22, 0.22, 0.05, -0.03, 0.08])
+    for n, seed, amplitudes in ((4, 7, (0.4e-3, 1.2e-3, 2.0e-3)), (8, 0, (0.6e-3, 1.4e-3, 2.2e-3))):
+        div = (n, n, n)
+        nodes, elements = build_structured_hex8_box((1.0, 1.0, 1.0), div)
+        phase = sphere_phase_map(div, draw_spheres(seed))
+        phased = PhasedMaterialModel("mortar__aggregate", (RVEPhase("matrix", mortar), RVEPhase("inclusion", aggregate)),
+                                     np.repeat(phase, 8), 2360.0)  # fmt: skip
+        model = StructuredHex8RVE(nodes, elements, div, phased, build_structured_hex8_periodic_constraint(nodes, div),
+                                  newton_c, element_phase_ids=phase, phase_names=("matrix", "inclusion"))  # fmt: skip
+        state = initialize_rve_state(model)
+        arrays, meta_steps = {"element_phase": phase}, []
+        for step, amp in enumerate(amplitudes):
+            macro = amp * direction
+            response = solve_rve_microequilibrium(
+                model, RVERequest(macro, 5.0e-6, update, MaterialResponseRequirements(tangent=True)), state)
+            a, sc = _rve_arrays(f"s{step}__", response, macro)
+            arrays.update(a)
+            meta_steps.append(sc)
+            state = response.state
+        meta = {"kind": "two_phase", "divisions": div, "seed": seed, "time_step": 5.0e-6, "steps": len(amplitudes),
+                "scalars": meta_steps, "newton": [25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, False],
+                "hill_mandel_power_scale": 1.0}  # fmt: skip
+        cases[f"rve_two_phase_{n}"] = (arrays, meta)
+    return cases
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--reference", default="/root/reference/src")
@@ -171,10 +262,11 @@ def main() -> None:
     cases = {}
     cases.update(make_j2_cases(data_mod, plasticity))
     cases.update(make_incremental_case(data_mod, plasticity))
+    cases.update(make_rve_cases())
     manifest = {}
     for name, (arrays, meta) in cases.items():
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
-        manifest[name] = meta
+        manifest[name] = json.loads(json.dumps(meta, default=lambda o: o.tolist() if hasattr(o, "tolist") else str(o)))
     failures = make_failure_cases(data_mod, plasticity, errors)
     (HERE / "j2_failures.json").write_text(json.dumps(failures, indent=1, sort_keys=True))
     (HERE / "manifest.json").write_text(json.dumps(manifest, indent=1, sort_keys=True))
