@@ -142,6 +142,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_j2vp_diagnose_point": (_I, [_P, _P, _I64, _D, _P, _P, _P, _P, _I64, _P, _P]),
     "cib_linear_elastic_update": (_I, [_D, _D, _I64, _D] + [_P] * 7),
     "cib_copy_rows_async": (_I, [_P, _I64, _P, _I64, _I64, _I64, _I, _P]),
+    "cib_hex8_geometry": (_I, [_I64] + [_P] * 6),
+    "cib_hex8_strains": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P, _P]),
+    "cib_hex8_internal_force": (_I, [_I64, _I64] + [_P] * 8),
+    "cib_hex8_tangent_csr": (_I, [_I64, _P, _P, _P, _I64, _P, _P, _P, _P, _P]),
     "cib_rve_residual": (_I, [_P] * 9),
     "cib_rve_gather": (_I, [_P] * 12),
     "cib_rve_pcg": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32] + [_P] * 5),

@@ -173,6 +173,32 @@ int cib_linear_elastic_update(double young_modulus, double poisson_ratio, int64_
                               double* tangent, double* free_energy, double* dissipation,
                               double* increment_diagnostics, void* stream);
 
+/* --- General Hex8 assembly (arbitrary nodes and connectivity) ---------------------------
+ * nodes (N,3) float64, elements (E,8) int64 in the lexicographic node order of the
+ * reference (src/fem/elements/lagrange.py:50-76), 2x2x2 Gauss rule.  Replaces the loops of
+ * src/fem/assembly/nonlinear_solid.py:391-493. */
+
+/* dN/dx per (element, Gauss point, node): grads (E*8*8*3), J*w (E*8); bad_count (device
+ * uint64) is incremented for every point with det J <= 0. */
+int cib_hex8_geometry(int64_t nelem, const double* nodes, const int64_t* elements, double* grads, double* jw,
+                      unsigned long long* bad_count, void* stream);
+
+/* strain (8E,6) = B u_e and, when rate is not NULL, rate (8E,6) = B (u_e - u_prev,e) / dt. */
+int cib_hex8_strains(int64_t nelem, const int64_t* elements, const double* grads, const double* u,
+                     const double* u_prev, double time_step, double* strain, double* rate, void* stream);
+
+/* Internal force (3N) = sum_e sum_q w B^T sigma: element nodal forces into fe (E*8*3,
+ * scratch), then a fixed-order gather per node over node_list[node_ptr[n] .. node_ptr[n+1])
+ * (entries 8 e + a). */
+int cib_hex8_internal_force(int64_t nelem, int64_t nnode, const double* grads, const double* jw, const double* stress,
+                            const int64_t* node_ptr, const int64_t* node_list, double* fe, double* force,
+                            void* stream);
+
+/* Tangent in CSR: element matrices into ke (E*24*24, scratch) from tangents (8E,6,6), then
+ * values[k] = sum of ke[csr_list[csr_ptr[k] .. csr_ptr[k+1])] in a fixed order. */
+int cib_hex8_tangent_csr(int64_t nelem, const double* grads, const double* jw, const double* tangent, int64_t nnz,
+                         const int64_t* csr_ptr, const int64_t* csr_list, double* ke, double* values, void* stream);
+
 /* --- Periodic structured Hex8 RVE batch ------------------------------------------------
  * A batch holds R structured periodic RVEs (unit-cell boxes of nx*ny*nz Hex8 elements).
  * RVE r owns elements [elem_offset, elem_offset + nx*ny*nz); its periodic node (class)
