@@ -140,7 +140,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_j2vp_update_soa_f32": (_I, [_P, _P, _I64, _I64, _D] + [_P] * 10),
     "cib_j2vp_update": (_I, [_P, _P, _I64, _D] + [_P] * 16),
     "cib_j2vp_diagnose_point": (_I, [_P, _P, _I64, _D, _P, _P, _P, _P, _I64, _P, _P]),
-    "cib_linear_elastic_update": (_I, [_D, _D, _I64, _D] + [_P] * 7),
+    "cib_linear_elastic_update": (_I, [_D, _D, _I64, _D] + [_P] * 8),
     "cib_copy_rows_async": (_I, [_P, _I64, _P, _I64, _I64, _I64, _I, _P]),
     "cib_hex8_geometry": (_I, [_I64] + [_P] * 6),
     "cib_hex8_strains": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P, _P]),

@@ -40,6 +40,25 @@ def test_library_exports_every_declared_symbol() -> None:
     assert set(_native.SIGNATURES) == declared
 
 
+def _declared_prototypes() -> dict[str, int]:
+    """Parameter count of every cib_ function prototype in the header."""
+    text = (REPO / "include" / "cib200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(cib_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_signatures_match_header_prototypes() -> None:
+    """Every ctypes binding passes exactly the C prototype's number of arguments."""
+    protos = _declared_prototypes()
+    assert set(protos) == set(_native.SIGNATURES)
+    for name, count in protos.items():
+        assert len(_native.SIGNATURES[name][1]) == count, (name, count, len(_native.SIGNATURES[name][1]))
+
+
 def test_struct_layouts_match_header() -> None:
     """ctypes mirrors of the C structs have the C sizes (no silent padding mismatch)."""
     assert ctypes.sizeof(_native.J2VPMaterialC) == 7 * 8
