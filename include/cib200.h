@@ -278,6 +278,24 @@ int cib_rve_pcg(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve
                 double* Ap, double rtol, int32_t maxit, int32_t* status, int32_t* iterations,
                 double* rel_residual, double* xnorm, void* stream);
 
+/* The solve of cib_rve_pcg for callers that cannot allocate device memory -- code running
+ * inside an allocator's or memory pool's own hooks, or under a host framework that forbids
+ * device allocations after start-up.  No counterpart in the reference (which has no GPU
+ * path).  The work vectors r, p and Ap live in one array compiled into the library:
+ * 3 x CIB_PCG_NOALLOC_MAX_VEC doubles (1.5 MiB), held by every GPU that loads the library
+ * until the process exits; nothing is allocated by the call.  vec_len is the length of b
+ * and x (doubles) and every system's vectors must lie inside it, as for cib_rve_pcg;
+ * vec_len > CIB_PCG_NOALLOC_MAX_VEC returns CIB_ERANGE without launching.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  All calls on a device share the array: calls that overlap
+ * on the GPU race and must not be issued; no content is carried from one call to the next.
+ * Outputs and status codes are those of cib_rve_pcg. */
+#define CIB_PCG_NOALLOC_MAX_VEC 65536
+int cib_rve_pcg_noalloc(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve, const int64_t* sys_off,
+                        const int32_t* active, int64_t vec_len, const double* b, const double* dinv, double* x,
+                        double rtol, int32_t maxit, int32_t* status, int32_t* iterations, double* rel_residual,
+                        double* xnorm, void* stream);
+
 /* Effective tangent (solver.py:438-461): right-hand sides K_we = T^T K A (6 columns per
  * RVE, layout [18*elem_offset + j*3*E_r + 3*c + d]) and K_ee = A^T K A (36 per RVE);
  * fe6 is scratch of 6*24*nelem doubles.  Then C = (K_ee - K_we^T S) / V from the PCG
