@@ -146,6 +146,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_hex8_strains": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P, _P]),
     "cib_hex8_internal_force": (_I, [_I64, _I64] + [_P] * 8),
     "cib_hex8_tangent_csr": (_I, [_I64, _P, _P, _P, _I64, _P, _P, _P, _P, _P]),
+    "cib_mlp_gemm": (_I, [ctypes.c_int32] * 4 + [_P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                          ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32,
+                          ctypes.c_int32, _P, _P]),
+    "cib_splitk_reduce": (_I, [ctypes.c_int32] * 3 + [_P, ctypes.c_int32, _P, ctypes.c_int32, _P]),
     "cib_rve_residual": (_I, [_P] * 9),
     "cib_rve_gather": (_I, [_P] * 12),
     "cib_rve_pcg": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32] + [_P] * 5),

@@ -46,41 +46,45 @@ class SphereLayout:
 
 
 def draw_spheres(seed: int, target_fraction: float = 0.4, r_min: float = 0.08, r_max: float = 0.15,
-                 lengths=(1.0, 1.0, 1.0), max_attempts: int = 200_000, batch: int = 512) -> SphereLayout:  # fmt: skip
-    """Seeded random sequential addition of non-overlapping periodic spheres.
+                 lengths=(1.0, 1.0, 1.0), candidates_per_sphere: int = 4096, batch: int = 512) -> SphereLayout:  # fmt: skip
+    """Seeded random placement of non-overlapping periodic spheres, largest first.
 
-    Candidates (radius, centre) are drawn in batches; each is tested, in draw order,
-    against every sphere accepted before it (minimum-image distance), so the result is
-    that of one-at-a-time rejection sampling of the same random stream."""
+    Radii U[r_min, r_max] are drawn until their total volume reaches the target fraction
+    of the box, then placed in decreasing size: each sphere takes the first of its seeded
+    candidate centres (drawn in batches) that clears every sphere placed before it
+    (minimum-image distance).  A sphere with no clear candidate is dropped, so the
+    achieved fraction can fall slightly short of the target near jamming."""
     rng = np.random.default_rng(seed)
     box = np.asarray(lengths, dtype=np.float64)
     volume = float(np.prod(box))
+    radii_drawn: list[float] = []
+    total = 0.0
+    while total < target_fraction * volume:
+        r = float(rng.uniform(r_min, r_max))
+        radii_drawn.append(r)
+        total += 4.0 / 3.0 * np.pi * r**3
+    order = sorted(radii_drawn, reverse=True)
     centres = np.zeros((0, 3))
     radii = np.zeros(0)
-    filled = 0.0
-    drawn = 0
-    while drawn < max_attempts and filled < target_fraction * volume:
-        m = min(batch, max_attempts - drawn)
-        r = rng.uniform(r_min, r_max, size=m)
-        c = rng.uniform(0.0, 1.0, size=(m, 3)) * box
-        drawn += m
-        if radii.size:
-            d = c[:, None, :] - centres[None, :, :]
-            d -= box * np.round(d / box)
-            clash = np.any(np.linalg.norm(d, axis=2) < r[:, None] + radii[None, :], axis=1)
-        else:
-            clash = np.zeros(m, dtype=bool)
-        for t in np.flatnonzero(~clash):
-            if filled >= target_fraction * volume:
-                break
+    for r in order:
+        placed = False
+        for _ in range(max(1, candidates_per_sphere // batch)):
+            c = rng.uniform(0.0, 1.0, size=(batch, 3)) * box
             if radii.size:
-                dd = centres - c[t]
-                dd -= box * np.round(dd / box)
-                if np.any(np.linalg.norm(dd, axis=1) < radii + r[t]):
-                    continue
-            centres = np.vstack([centres, c[t]])
-            radii = np.append(radii, r[t])
-            filled += 4.0 / 3.0 * np.pi * r[t] ** 3
+                d = c[:, None, :] - centres[None, :, :]
+                d -= box * np.round(d / box)
+                ok = ~np.any(np.einsum("ijk,ijk->ij", d, d) < (radii[None, :] + r) ** 2, axis=1)
+            else:
+                ok = np.ones(batch, dtype=bool)
+            hit = np.flatnonzero(ok)
+            if hit.size:
+                centres = np.vstack([centres, c[hit[0]]])
+                radii = np.append(radii, r)
+                placed = True
+                break
+        if not placed:
+            continue
+    filled = float(np.sum(4.0 / 3.0 * np.pi * radii**3))
     return SphereLayout(centres, radii, target_fraction, filled / volume)
 
 

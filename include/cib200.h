@@ -314,6 +314,29 @@ int cib_rve_response(const cib_rve_batch* batch, const double* time_step, const 
                      const double* w, const double* w_n, const int32_t* active, double* sums, double* point_out,
                      double* diagnostics, void* stream);
 
+/* --- Tensor-core MLP GEMM (recurrent material surrogate) --------------------------------
+ * C[M x N] = A[M x K] . B[N x K]^T, A and B bf16 row-major (leading dimensions lda, ldb,
+ * multiples of 8; 16-byte aligned), fp32 accumulation in tensor memory (tcgen05.mma).
+ * N in {16, 32, ..., 128}, K a multiple of 16.  B must hold N rows.  Epilogues:
+ *   0 C = acc (fp32)                      1 C = acc + bias (fp32)
+ *   2 Z = acc + bias (fp32), H = gelu(Z) (bf16), optional Ht[n * ldht + row_offset + m] = H
+ *   3 H = acc * gelu'(Z) (bf16), optional Ht as above
+ *   4 fp32 partial sums per K slice into C[(slice * M + m) * ldc + n] (splits > 1), reduced
+ *     by cib_splitk_reduce in a fixed order.
+ * err (device uint32) becomes 1 if a tensor-core completion wait exceeds 2 s (the CTA then
+ * returns after releasing its tensor memory).  No reference counterpart: the reference
+ * runs its surrogate through torch.nn.Linear (src/concrete_impact/nn/models/rve_rno.py:63-93). */
+#define CIB_EPI_F32 0
+#define CIB_EPI_BIAS_F32 1
+#define CIB_EPI_BIAS_GELU 2
+#define CIB_EPI_GELU_BWD 3
+#define CIB_EPI_PARTIAL 4
+int cib_mlp_gemm(int32_t epilogue, int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const void* B,
+                 int32_t ldb, int32_t splits, const float* bias, float* C, int32_t ldc, float* Z, int32_t ldz, void* H,
+                 int32_t ldh, void* Ht, int32_t ldht, int32_t row_offset, unsigned int* err, void* stream);
+int cib_splitk_reduce(int32_t M, int32_t N, int32_t splits, const float* partial, int32_t ldc, float* out, int32_t ldo,
+                      void* stream);
+
 /* Strided host<->device copy of `rows` rows of `row_bytes` bytes (one cudaMemcpy2DAsync);
  * kind 1 = host to device, 2 = device to host, 3 = device to device. */
 int cib_copy_rows_async(void* dst, int64_t dst_pitch, const void* src, int64_t src_pitch, int64_t row_bytes,
