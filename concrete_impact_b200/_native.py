@@ -150,6 +150,14 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
                           ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32, _P, ctypes.c_int32,
                           ctypes.c_int32, _P, _P]),
     "cib_splitk_reduce": (_I, [ctypes.c_int32] * 3 + [_P, ctypes.c_int32, _P, ctypes.c_int32, _P]),
+    "cib_rno_input": (_I, [ctypes.c_int32, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P]),
+    "cib_rno_forward_tail": (_I, [ctypes.c_int32, _P, _P, _P, _P, _P, _P, ctypes.c_float, _P, _P]),
+    "cib_rno_backward_head": (_I, [ctypes.c_int32, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P]),
+    "cib_rno_backward_tail": (_I, [ctypes.c_int32, _P, _P, _P, _P]),
+    "cib_row_sum_bf16": (_I, [ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int32, _P, _P]),
+    "cib_adam_step": (_I, [ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P] + [ctypes.c_float] * 4
+                      + [_P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P]),
+    "cib_counter_increment": (_I, [_P, _P]),
     "cib_rve_residual": (_I, [_P] * 9),
     "cib_rve_gather": (_I, [_P] * 12),
     "cib_rve_pcg": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32] + [_P] * 5),

@@ -11,7 +11,7 @@
 // and applies one of:
 //   EPI_F32        C = acc                                   (fp32 out)
 //   EPI_BIAS_F32   C = acc + bias                            (fp32 out; output layer)
-//   EPI_BIAS_GELU  Z = acc + bias (fp32), H = gelu(Z) (bf16), optional H^T (bf16)
+//   EPI_BIAS_GELU  Z = acc + bias (fp32, optional), H = gelu(Z) (bf16), optional H^T (bf16)
 //   EPI_GELU_BWD   dZ = acc * gelu'(Z) (bf16), optional dZ^T (bf16)
 //   EPI_PARTIAL    fp32 partial of this K slice, reduced later in a fixed order
 #include <cuda_bf16.h>
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) umma_gemm_kernel(const GemmArgs 
             a.C[(size_t)m * a.ldc + n] = acc + a.bias[n];
           } else if (EPI == EPI_BIAS_GELU) {
             const float z = acc + a.bias[n];
-            a.Z[(size_t)m * a.ldz + n] = z;
+            if (a.Z) a.Z[(size_t)m * a.ldz + n] = z;
             const __nv_bfloat16 h = __float2bfloat16_rn(gelu(z));
             a.H[(size_t)m * a.ldh + n] = h;
             if (a.Ht) a.Ht[(size_t)n * a.ldht + a.row_offset + m] = h;
@@ -276,7 +276,7 @@ extern "C" int cib_mlp_gemm(int32_t epilogue, int32_t M, int32_t N, int32_t K, c
       if (!C || (epilogue == EPI_BIAS_F32 && !bias) || ny != 1) return CIB_EINVAL;
       break;
     case EPI_BIAS_GELU:
-      if (!bias || !Z || !H || ny != 1) return CIB_EINVAL;
+      if (!bias || !H || ny != 1) return CIB_EINVAL;
       break;
     case EPI_GELU_BWD:
       if (!Z || !H || ny != 1) return CIB_EINVAL;

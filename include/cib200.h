@@ -319,7 +319,8 @@ int cib_rve_response(const cib_rve_batch* batch, const double* time_step, const 
  * multiples of 8; 16-byte aligned), fp32 accumulation in tensor memory (tcgen05.mma).
  * N in {16, 32, ..., 128}, K a multiple of 16.  B must hold N rows.  Epilogues:
  *   0 C = acc (fp32)                      1 C = acc + bias (fp32)
- *   2 Z = acc + bias (fp32), H = gelu(Z) (bf16), optional Ht[n * ldht + row_offset + m] = H
+ *   2 Z = acc + bias (fp32; Z may be NULL), H = gelu(Z) (bf16), optional
+ *     Ht[n * ldht + row_offset + m] = H
  *   3 H = acc * gelu'(Z) (bf16), optional Ht as above
  *   4 fp32 partial sums per K slice into C[(slice * M + m) * ldc + n] (splits > 1), reduced
  *     by cib_splitk_reduce in a fixed order.
@@ -336,6 +337,31 @@ int cib_mlp_gemm(int32_t epilogue, int32_t M, int32_t N, int32_t K, const void* 
                  int32_t ldh, void* Ht, int32_t ldht, int32_t row_offset, unsigned int* err, void* stream);
 int cib_splitk_reduce(int32_t M, int32_t N, int32_t splits, const float* partial, int32_t ldc, float* out, int32_t ldo,
                       void* stream);
+
+/* --- Recurrent surrogate (RNO) elementwise kernels ------------------------------------
+ * Per time step for B paths: x = [strain 6, strain rate 6, latent 6, zeros 14] (bf16,
+ * B x 32, optional transpose Xt[c * ldxt + row_offset + p]); output Y (B x 16 fp32):
+ * normalised stress (0..5) and latent rate (6..11); z' = z + coef * Y[:, 6:12] (the
+ * forward-Euler latent step of src/concrete_impact/nn/models/rve_rno.py:383-387);
+ * gY = loss_scale * 2 (Y[:, 0:6] - target); loss_part[block] = sum of squared errors
+ * (256 paths per block). */
+int cib_rno_input(int32_t B, const float* strain, const float* rate, const float* z, void* X, void* Xt, int32_t ldxt,
+                  int32_t row_offset, void* stream);
+int cib_rno_forward_tail(int32_t B, const float* Y, const float* target, const float* coef, const float* z,
+                         float* z_next, float* gY, float loss_scale, double* loss_part, void* stream);
+/* dY = [gY, coef * dz_next, 0] (bf16, B x 16) and its transpose; dz = dz_next + dX[:, 12:18]. */
+int cib_rno_backward_head(int32_t B, const float* gY, const float* coef, const float* dz_next, void* dY, void* dYt,
+                          int32_t lddyt, int32_t row_offset, void* stream);
+int cib_rno_backward_tail(int32_t B, const float* dz_next, const float* dX, float* dz, void* stream);
+/* out[n] = sum over r < R of X[n * ld + r] (bf16 rows; bias gradients). */
+int cib_row_sum_bf16(int32_t rows, int32_t R, const void* X, int32_t ld, float* out, void* stream);
+/* Adam with bias correction on fp32 weights (rows x cols), refreshing the bf16 copy Wb and
+ * its transpose Wt when given (NULL skips).  The step number is read from device memory
+ * (so a captured graph can replay it); cib_counter_increment adds one to it. */
+int cib_adam_step(int32_t rows, int32_t cols, float* w, const float* g, float* m, float* v, float lr, float beta1,
+                  float beta2, float eps, const int32_t* step, void* Wb, int32_t ldb, void* Wt, int32_t ldt,
+                  void* stream);
+int cib_counter_increment(int32_t* counter, void* stream);
 
 /* Strided host<->device copy of `rows` rows of `row_bytes` bytes (one cudaMemcpy2DAsync);
  * kind 1 = host to device, 2 = device to host, 3 = device to device. */
