@@ -158,6 +158,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_adam_step": (_I, [ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P] + [ctypes.c_float] * 4
                       + [_P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P]),
     "cib_counter_increment": (_I, [_P, _P]),
+    "cib_verlet_predict": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P]),
+    "cib_verlet_correct": (_I, [_I64, _P, _D, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     "cib_rve_residual": (_I, [_P] * 9),
     "cib_rve_gather": (_I, [_P] * 12),
     "cib_rve_pcg": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32] + [_P] * 5),

@@ -1,0 +1,312 @@
+"""Explicit FE^2 impact dynamics on the GPU: macro Hex8 bar, velocity Verlet, RVE or RNO points.
+
+Restates the reference's explicit material dynamics (solve_material_explicit,
+src/fem/dynamics/material.py:89-297: lumped row-sum mass, velocity Verlet, homogeneous
+Dirichlet DOFs, material update without tangent each step), its CFL bound
+(src/fem/dynamics/stability.py:34-48), the half-sine pressure pulse
+(src/concrete_impact/benchmarks/dynamic_viscoplastic.py:147-170) and the uniform boundary
+pressure (src/fem/assembly/load.py:40-77), with the macro kernels of ``csrc/hex8.cu`` and
+``csrc/fe2.cu``.  The macro material at the integration points is either
+
+* ``DirectRVEPoints`` -- one periodic RVE per macro point, all solved in device batches
+  (the reference's RVEHomogenizedMaterial), or
+* ``RNOPoints`` -- the recurrent surrogate with one latent state per point, behind an error
+  gate: a point whose surrogate input leaves the training envelope falls back to a direct
+  RVE solve (fallback pool of RVEs; its RVE starts with a catch-up step that loads it
+  proportionally to the current macro strain over the elapsed time).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native
+from .assembly import MaterialAssemblyCache, build_hex8_material_assembly_cache
+from .materials import MaterialPointRequest, MaterialState, MaterialUpdateSettings
+from .rno import RNOSurrogate
+from .rve import RS_SIGMA, NonlinearNewtonSettings, RVEBatch, StructuredHex8RVE, build_structured_hex8_box, solve_batch_step
+
+
+@dataclass
+class MacroBar:
+    """Structured macro Hex8 bar with the left face fixed and a pressure on the right face."""
+
+    nodes: np.ndarray
+    elements: np.ndarray
+    divisions: tuple[int, int, int]
+    lengths: tuple[float, float, float]
+    density: float
+    fixed: torch.Tensor  # (3N,) uint8
+    unit_force: torch.Tensor  # (3N,) nodal force of a unit pressure
+    mass: torch.Tensor  # (3N,) lumped row-sum mass
+    cache: MaterialAssemblyCache = field(repr=False)
+
+    @property
+    def points(self) -> int:
+        return 8 * int(self.elements.shape[0])
+
+    @property
+    def min_edge(self) -> float:
+        return float(min(l / n for l, n in zip(self.lengths, self.divisions)))
+
+
+def build_macro_bar(divisions=(64, 16, 16), lengths=(0.64, 0.16, 0.16), density: float = 2400.0) -> MacroBar:
+    """Bar with x the long axis: x = 0 face fixed, unit pressure on the x = L face."""
+    dev = _native.require_cuda()
+    nodes, elements = build_structured_hex8_box(tuple(lengths), tuple(divisions))
+    n = nodes.shape[0]
+    left = np.isclose(nodes[:, 0], 0.0)
+    right = np.isclose(nodes[:, 0], lengths[0])
+    fixed = np.zeros(3 * n, dtype=np.uint8)
+    fixed[(3 * np.flatnonzero(left)[:, None] + np.arange(3)).ravel()] = 1
+    # uniform traction -p * outward normal (+x) split equally over the 4 nodes of each face quad
+    ny, nz = divisions[1], divisions[2]
+    face_area = (lengths[1] / ny) * (lengths[2] / nz)
+    count = np.zeros(n)
+    jr = np.rint(nodes[:, 1] / (lengths[1] / ny)).astype(int)
+    kr = np.rint(nodes[:, 2] / (lengths[2] / nz)).astype(int)
+    inner_y = np.where((jr == 0) | (jr == ny), 1, 2)
+    inner_z = np.where((kr == 0) | (kr == nz), 1, 2)
+    count[right] = (inner_y * inner_z)[right]
+    unit = np.zeros(3 * n)
+    unit[3 * np.flatnonzero(right)] = -face_area / 4.0 * count[right]
+    vol = float(np.prod([l / d for l, d in zip(lengths, divisions)]))
+    mass_node = np.zeros(n)
+    np.add.at(mass_node, elements.reshape(-1), density * vol / 8.0)
+    cache = build_hex8_material_assembly_cache(nodes, elements)
+    t = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt, device=dev)  # noqa: E731
+    return MacroBar(nodes, elements, tuple(divisions), tuple(lengths), density, t(fixed, torch.uint8), t(unit),
+                    t(np.repeat(mass_node, 3)), cache)  # fmt: skip
+
+
+def half_sine_pressure(time: float, amplitude: float = 50.0e6, duration: float = 50.0e-6) -> float:
+    """Half-sine pulse amplitude * sin(pi t / duration) for 0 <= t <= duration, else 0."""
+    return amplitude * math.sin(math.pi * time / duration) if 0.0 <= time <= duration else 0.0
+
+
+def stable_time_step(bar: MacroBar, wave_speed: float, safety: float = 0.5) -> float:
+    """CFL bound safety * h_min / c_p."""
+    return safety * bar.min_edge / wave_speed
+
+
+# --------------------------------------------------------------------------------------
+# Macro materials.
+
+
+class MaterialPoints:
+    """A material model of the point protocol (J2, linear elastic, phased) at every macro
+    point, with its state on the device; the reference's solve_material_explicit with a
+    plain constitutive law."""
+
+    def __init__(self, material, n_points: int, update_settings: MaterialUpdateSettings) -> None:
+        dev = _native.require_cuda()
+        self.material = material
+        self.settings = update_settings
+        init = material.initialize_state(n_points)
+        self.state = MaterialState({k: torch.as_tensor(v, device=dev) for k, v in init.variables.items()})
+        self.trial = self.state
+
+    def stress(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
+        req = MaterialPointRequest(strain, rate, dt, "three_dimensional", self.settings)
+        resp = self.material.update(req, self.state)
+        self.trial = resp.state
+        return resp.stresses
+
+    def commit(self) -> None:
+        self.state = self.trial
+
+
+class DirectRVEPoints:
+    """One RVE per macro point, solved in device batches of at most ``chunk`` RVEs."""
+
+    def __init__(self, model: StructuredHex8RVE, n_points: int, update_settings: MaterialUpdateSettings,
+                 precision: int = 32, chunk: int = 16384) -> None:  # fmt: skip
+        self.model = model
+        self.n = n_points
+        self.settings = update_settings
+        self.batches = [RVEBatch([model] * min(chunk, n_points - s), precision=precision)
+                        for s in range(0, n_points, chunk)]  # fmt: skip
+        self.starts = list(range(0, n_points, chunk))
+        self.volume = float(self.batches[0].volumes[0])
+        self.newton_iterations = 0
+
+    def stress(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
+        out = torch.empty((self.n, 6), dtype=torch.float64, device=strain.device)
+        for s, b in zip(self.starts, self.batches):
+            sl = slice(s, s + b.nrve)
+            b.macro.copy_(strain[sl])
+            b.dt.fill_(dt)
+            res = solve_batch_step(b, self.model.newton_settings, self.settings, False)
+            self.newton_iterations = max(self.newton_iterations, int(res.newton_iterations.max()))
+            b.response(b.batch_struct(self.settings), b.w, None, None)
+            out[sl] = b.sums[:, RS_SIGMA : RS_SIGMA + 6] / self.volume
+        return out
+
+    def commit(self) -> None:
+        for b in self.batches:
+            b.commit()
+
+
+class RNOPoints:
+    """The surrogate at every macro point, with an input-envelope gate and a direct fallback.
+
+    ``envelope`` = (max |normalised strain|, max |normalised rate|) seen in training; a point
+    whose input exceeds ``envelope_factor`` times it is flagged and solved by a fallback RVE
+    from then on (at most ``fallback_capacity`` points).
+    """
+
+    def __init__(self, rno: RNOSurrogate, n_points: int, envelope: tuple[float, float],
+                 model: StructuredHex8RVE | None = None, update_settings: MaterialUpdateSettings | None = None,
+                 envelope_factor: float = 1.05, fallback_capacity: int = 2048, precision: int = 32) -> None:  # fmt: skip
+        self.rno = rno
+        self.n = n_points
+        dev = rno.device
+        self.z = torch.zeros((n_points, 6), dtype=torch.float32, device=dev)
+        self.z_next = self.z
+        self.envelope = envelope
+        self.factor = envelope_factor
+        self.model = model
+        self.settings = update_settings
+        self.buffers = None
+        self.flagged = torch.zeros(n_points, dtype=torch.bool, device=dev)
+        self.slot_of = torch.full((n_points,), -1, dtype=torch.int64, device=dev)
+        self.slots_used = 0
+        self.pool = RVEBatch([model] * fallback_capacity, precision=precision) if model is not None else None
+        self.capacity = fallback_capacity if model is not None else 0
+        self.pool_points = torch.full((self.capacity,), -1, dtype=torch.int64, device=dev)
+        self.time = 0.0
+        self.fallback_steps = 0
+        self.pool_dt_override: tuple[int, int] | None = None
+
+    def stress(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
+        s = self.rno.scales
+        coef = torch.full((self.n,), dt / self.rno.config.tau_ref, dtype=torch.float32, device=strain.device)
+        out, z_next, self.buffers = self.rno.predict(strain, rate, self.z, coef, self.buffers)
+        self.z_next = z_next
+        stress = out.double()
+        if self.pool is None:
+            return stress
+        over = ((strain.abs() / s.strain).amax(dim=1) > self.factor * self.envelope[0]) | (
+            (rate.abs() / s.rate).amax(dim=1) > self.factor * self.envelope[1])  # fmt: skip
+        new = over & ~self.flagged
+        if bool(new.any()):
+            self._admit(torch.nonzero(new).flatten(), strain)
+        if self.slots_used:
+            used = slice(0, self.slots_used)
+            pts = self.pool_points[used]
+            self.pool.macro[used] = strain[pts]
+            fresh = self.pool_dt_override
+            self.pool.dt[used] = dt
+            if fresh is not None:
+                self.pool.dt[fresh[0]:fresh[1]] = max(self.time + dt, dt)
+            self.pool_dt_override = None
+            mask = np.zeros(self.capacity, dtype=bool)
+            mask[: self.slots_used] = True
+            solve_batch_step(self.pool, self.model.newton_settings, self.settings, False, live_mask=mask)
+            self.pool.response(self.pool.batch_struct(self.settings), self.pool.w, None, None)
+            vol = float(self.pool.volumes[0])
+            stress[pts] = self.pool.sums[used, RS_SIGMA : RS_SIGMA + 6] / vol
+            self.fallback_steps += 1
+        return stress
+
+    def _admit(self, points: torch.Tensor, strain: torch.Tensor) -> None:
+        """Give newly flagged points a fallback RVE from the zero state; the first solve of
+        the slot is a catch-up step over the elapsed time."""
+        room = self.capacity - self.slots_used
+        if points.numel() > room:
+            raise RuntimeError(f"RNO error gate flagged more points than the fallback pool holds ({self.capacity}).")
+        a, b = self.slots_used, self.slots_used + int(points.numel())
+        self.pool_points[a:b] = points
+        self.flagged[points] = True
+        self.slot_of[points] = torch.arange(a, b, device=points.device)
+        p = self.pool
+        E = int(p.elem_counts[0])
+        g0, g1 = 8 * E * a, 8 * E * b
+        p.ep_n[:, g0:g1] = 0
+        p.q_n[g0:g1] = 0
+        p.vpm_n[g0:g1] = 0
+        p.w_n[3 * E * a : 3 * E * b] = 0
+        p.macro_n[a:b] = 0
+        self.slots_used = b
+        self.pool_dt_override = (a, b)
+
+    def commit(self) -> None:
+        self.z = self.z_next.clone()
+        if self.slots_used:
+            self.pool.commit()
+
+    def advance_time(self, dt: float) -> None:
+        self.time += dt
+
+
+class ExplicitFE2:
+    """Velocity-Verlet macro dynamics with a macro-point material (direct RVEs or RNO)."""
+
+    def __init__(self, bar: MacroBar, material, dt: float, pressure=half_sine_pressure) -> None:
+        self.bar = bar
+        self.material = material
+        self.dt = float(dt)
+        self.pressure = pressure
+        self.lib = _native.load_library()
+        dev = bar.fixed.device
+        n3 = bar.fixed.numel()
+        z = lambda: torch.zeros(n3, dtype=torch.float64, device=dev)  # noqa: E731
+        self.u, self.v, self.a = z(), z(), z()
+        self.u_next, self.v_next, self.a_next = z(), z(), z()
+        npts = bar.points
+        self.strain = torch.zeros((npts, 6), dtype=torch.float64, device=dev)
+        self.rate = torch.zeros((npts, 6), dtype=torch.float64, device=dev)
+        self.fe = torch.empty(npts * 3, dtype=torch.float64, device=dev)
+        self.f_int = z()
+        self.time = 0.0
+        self.step_count = 0
+        self.last_stress: torch.Tensor | None = None
+
+    def _strains(self, u: torch.Tensor, u_prev: torch.Tensor) -> None:
+        c = self.bar.cache
+        code = self.lib.cib_hex8_strains(int(c.elements.shape[0]), c.elements.data_ptr(), c.grads.data_ptr(),
+                                         u.data_ptr(), u_prev.data_ptr(), self.dt, self.strain.data_ptr(),
+                                         self.rate.data_ptr(), _native.stream_ptr())  # fmt: skip
+        _native.check(code, "cib_hex8_strains")
+
+    def _internal_force(self, stress: torch.Tensor) -> None:
+        c = self.bar.cache
+        code = self.lib.cib_hex8_internal_force(int(c.elements.shape[0]), c.node_count, c.grads.data_ptr(),
+                                                c.jw.data_ptr(), stress.data_ptr(), c.node_ptr.data_ptr(),
+                                                c.node_list.data_ptr(), self.fe.data_ptr(), self.f_int.data_ptr(),
+                                                _native.stream_ptr())  # fmt: skip
+        _native.check(code, "cib_hex8_internal_force")
+
+    def step(self) -> None:
+        """One velocity-Verlet step (material.py:195-219)."""
+        sp = _native.stream_ptr()
+        n = self.u.numel()
+        _native.check(self.lib.cib_verlet_predict(n, self.u.data_ptr(), self.v.data_ptr(), self.a.data_ptr(),
+                                                  self.bar.fixed.data_ptr(), self.dt, self.u_next.data_ptr(), sp),
+                      "cib_verlet_predict")  # fmt: skip
+        self._strains(self.u_next, self.u)
+        stress = self.material.stress(self.strain, self.rate, self.dt).contiguous()
+        self._internal_force(stress)
+        t1 = self.time + self.dt
+        _native.check(self.lib.cib_verlet_correct(n, self.bar.unit_force.data_ptr(), float(self.pressure(t1)),
+                                                  self.f_int.data_ptr(), self.bar.mass.data_ptr(),
+                                                  self.bar.fixed.data_ptr(), self.dt, self.a.data_ptr(),
+                                                  self.v.data_ptr(), self.a_next.data_ptr(), self.v_next.data_ptr(), sp),
+                      "cib_verlet_correct")  # fmt: skip
+        self.material.commit()
+        if hasattr(self.material, "advance_time"):
+            self.material.advance_time(self.dt)
+        self.u, self.u_next = self.u_next, self.u
+        self.v, self.v_next = self.v_next, self.v
+        self.a, self.a_next = self.a_next, self.a
+        self.time = t1
+        self.step_count += 1
+        self.last_stress = stress
+
+    def run(self, steps: int) -> None:
+        for _ in range(steps):
+            self.step()

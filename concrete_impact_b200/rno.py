@@ -127,6 +127,7 @@ class RNOSurrogate:
             self.layers.append(self._make_layer(w, b))
         self.step = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.learning_rate = float(config.learning_rate)
         self._window: dict | None = None
         self._graph: torch.cuda.CUDAGraph | None = None
 
@@ -243,12 +244,19 @@ class RNOSurrogate:
         for L in self.layers:
             out, inp = L.w.shape
             _check(lib.cib_adam_step(out, inp, L.w.data_ptr(), L.gw.data_ptr(), L.mw.data_ptr(), L.vw.data_ptr(),
-                                     c.learning_rate, c.beta1, c.beta2, c.eps, self.step.data_ptr(), L.wb.data_ptr(),
+                                     self.learning_rate, c.beta1, c.beta2, c.eps, self.step.data_ptr(), L.wb.data_ptr(),
                                      inp, L.wt.data_ptr(), out, sp), "cib_adam_step")  # fmt: skip
             _check(lib.cib_adam_step(1, out, L.b.data_ptr(), L.gb.data_ptr(), L.mb.data_ptr(), L.vb.data_ptr(),
-                                     c.learning_rate, c.beta1, c.beta2, c.eps, self.step.data_ptr(), None, 0, None, 0,
+                                     self.learning_rate, c.beta1, c.beta2, c.eps, self.step.data_ptr(), None, 0, None, 0,
                                      sp), "cib_adam_step")  # fmt: skip
         # padded rows/columns stay zero: their gradients are identically zero
+
+    def set_learning_rate(self, lr: float) -> None:
+        """Change Adam's step size; the captured training graph holds it as a launch
+        argument, so it is captured again at the next replay."""
+        if float(lr) != self.learning_rate:
+            self.learning_rate = float(lr)
+            self._graph = None
 
     def window_step(self, T: int, B: int, train: bool = True) -> None:
         """Forward (+ backward, gradients and Adam when ``train``) on the loaded window."""
@@ -285,8 +293,9 @@ class RNOSurrogate:
         return float(w["loss_part"].sum().item()) / float(w["B"] * w["T"] * 6)
 
     # -- training -----------------------------------------------------------------------
-    def fit(self, data: RNODataset, epochs: int, graph: bool = True, log=None) -> list[float]:
-        """Train on ``data`` (device-resident); returns the mean loss per epoch."""
+    def fit(self, data: RNODataset, epochs: int, graph: bool = True, log=None, lr_schedule=None) -> list[float]:
+        """Train on ``data`` (device-resident); returns the mean loss per epoch.
+        ``lr_schedule(epoch)``, when given, sets the step size of each epoch."""
         c = self.config
         P, T = data.paths, data.steps
         rates = data.rates()
@@ -302,6 +311,8 @@ class RNOSurrogate:
         gen = torch.Generator(device="cpu").manual_seed(c.seed)
         history = []
         for epoch in range(epochs):
+            if lr_schedule is not None:
+                self.set_learning_rate(lr_schedule(epoch))
             perm = torch.randperm(P, generator=gen)
             losses = []
             for start in range(0, P - B + 1, B):

@@ -378,11 +378,15 @@ class RVEBatch:
         descs, phase_arrays, offsets = [], [], []
         off = 0
         self.max_nxy = 1
+        checked: dict[int, tuple] = {}
         for m in models:
-            ph, el_phase = _phases_of(m)
-            if [type(x[1]) for x in ph] != [type(x[1]) for x in phases0] or [x[1] for x in ph] != [x[1] for x in phases0]:
-                raise ValueError("all RVEs of a batch must share the phase materials")
-            hx, hy, hz = _check_structured(m)
+            key = id(m)
+            if key not in checked:  # a model object repeated in the batch is validated once
+                ph, el_phase = _phases_of(m)
+                if [type(x[1]) for x in ph] != [type(x[1]) for x in phases0] or [x[1] for x in ph] != [x[1] for x in phases0]:
+                    raise ValueError("all RVEs of a batch must share the phase materials")
+                checked[key] = (el_phase, _check_structured(m))
+            el_phase, (hx, hy, hz) = checked[key]
             nx, ny, nz = m.divisions
             descs.append(_native.RVEDescC(nx, ny, nz, 0, off, hx, hy, hz))
             phase_arrays.append(el_phase)
@@ -553,17 +557,20 @@ def solve_batch_step(
     point_out: torch.Tensor | None = None,
     diag: torch.Tensor | None = None,
     failure_context: Callable[[int, int], Exception] | None = None,
+    live_mask: np.ndarray | None = None,
 ) -> BatchStepResult:
     """Solve the microequilibrium of every RVE of the batch from its committed state.
 
     ``batch.macro`` / ``batch.dt`` hold the request; ``batch.w`` starts at the committed
     fluctuation.  On success the trial state of every RVE is its converged state (not yet
-    committed) and ``batch.sums`` its homogenisation sums.
+    committed).  ``live_mask`` restricts the solve to some RVEs; the others are left
+    untouched and stay inactive (``batch.active``) for the response and tangent kernels.
     """
     R = batch.nrve
     b = batch.batch_struct(update_settings)
     batch.w.copy_(batch.w_n)
-    done = np.zeros(R, dtype=bool)
+    done = np.zeros(R, dtype=bool) if live_mask is None else ~np.asarray(live_mask, dtype=bool)
+    final_active = None if live_mask is None else np.asarray(live_mask, dtype=bool).copy()
     init_norm = np.full(R, np.nan)
     last_inc = np.full(R, np.inf)
     backtracks = np.zeros(R, dtype=np.int64)
@@ -571,7 +578,7 @@ def solve_batch_step(
     res_out = np.zeros(R)
     tol_out = np.zeros(R)
     pcg_total = np.zeros(R, dtype=np.int64)
-    batch.active.fill_(1)
+    _set_active(batch, ~done)
     ns = newton
     for iteration in range(ns.max_iterations + 1):
         batch.residual(b, batch.w, None, None)
@@ -618,7 +625,10 @@ def solve_batch_step(
         _set_active(batch, live)
         _axpy_commit(batch, b)
         last_inc = np.where(live, steps * xnorm, last_inc)
-    batch.active.fill_(1)
+    if final_active is None:
+        batch.active.fill_(1)
+    else:
+        _set_active(batch, final_active)
     return BatchStepResult(iters_out, backtracks, res_out, tol_out, pcg_total)
 
 

@@ -221,6 +221,17 @@ def default_newton(armijo: bool = False) -> NonlinearNewtonSettings:
     return NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=armijo))
 
 
+def fp32_newton(stress_scale: float = 20.0e6, face_area: float = 1.0, armijo: bool = False) -> NonlinearNewtonSettings:
+    """Newton settings for FP32 element kernels.  The residual of an FP32 stress field has a
+    roundoff floor of about 1e-7 of the element forces, which a tolerance relative to a small
+    step's initial residual can fall below; the absolute tolerance is therefore 1e-6 of the
+    traction resultant ``stress_scale`` * ``face_area`` (20 N on a unit cell at 20 MPa)."""
+    from .rve import ArmijoSettings
+
+    return NonlinearNewtonSettings(25, 1.0e-6 * stress_scale * face_area, 1.0e-6, 1.0e-14, 1.0e-6,
+                                   ArmijoSettings(enabled=armijo))  # fmt: skip
+
+
 def uniaxial_path(steps: int = 100, final_strain: float = -5.0e-3, rate: float = 10.0) -> tuple[np.ndarray, np.ndarray]:
     """Times and prescribed xx strain of the uniaxial compression ramp."""
     exx = np.linspace(0.0, final_strain, steps + 1)

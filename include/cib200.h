@@ -363,6 +363,16 @@ int cib_adam_step(int32_t rows, int32_t cols, float* w, const float* g, float* m
                   void* stream);
 int cib_counter_increment(int32_t* counter, void* stream);
 
+/* --- Explicit macro dynamics (FE^2) ---------------------------------------------------
+ * Velocity-Verlet step of src/fem/dynamics/material.py:164-219 with a lumped mass and
+ * homogeneous Dirichlet DOFs (fixed[i] != 0): predictor u' = u + dt v + dt^2/2 a, then
+ * corrector a' = (load_scale f_unit - f_int) / m, v' = v + dt/2 (a + a'). */
+int cib_verlet_predict(int64_t n, const double* u, const double* v, const double* a, const uint8_t* fixed, double dt,
+                       double* u_next, void* stream);
+int cib_verlet_correct(int64_t n, const double* f_unit, double load_scale, const double* f_int, const double* mass,
+                       const uint8_t* fixed, double dt, const double* a, const double* v, double* a_next,
+                       double* v_next, void* stream);
+
 /* Strided host<->device copy of `rows` rows of `row_bytes` bytes (one cudaMemcpy2DAsync);
  * kind 1 = host to device, 2 = device to host, 3 = device to device. */
 int cib_copy_rows_async(void* dst, int64_t dst_pitch, const void* src, int64_t src_pitch, int64_t row_bytes,
