@@ -37,18 +37,25 @@ METRIC = "Gauss-point updates/s (batched J2 Perzyna return map with consistent t
 UNIT = "GP/s"
 WORKLOAD = "isolated batched return map, 16,777,216 GP SoA, FP64 state, tangent written"
 FALLBACK_HBM_GBS = 6650.0
+# (timed steps, warm-up steps) per workload when not given on the command line
+WORKLOAD_DEFAULTS = {"return_map": (200, 5), "rve_path": (100, 3), "rve_batch": (5, 3)}
 
 
 def parse_args() -> argparse.Namespace:
     parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=200)
-    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--steps", type=int, default=None)
+    parser.add_argument("--warmup", type=int, default=None)
+    parser.add_argument("--workload", choices=tuple(WORKLOAD_DEFAULTS), default="return_map")
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--points", type=int, default=N_POINTS, help=argparse.SUPPRESS)
     parser.add_argument("--e2e-steps", type=int, default=3)
     parser.add_argument("--no-cpu-baseline", action="store_true", help=argparse.SUPPRESS)
-    return parser.parse_args()
+    args = parser.parse_args()
+    steps, warmup = WORKLOAD_DEFAULTS[args.workload]
+    args.steps = steps if args.steps is None else args.steps
+    args.warmup = warmup if args.warmup is None else args.warmup
+    return args
 
 
 # ---------------------------------------------------------------------------------------
@@ -403,7 +410,11 @@ def run_ours(args: argparse.Namespace) -> None:
 def main() -> None:
     args = parse_args()
     sys.path.insert(0, str(REPO))
-    if args.impl == "reference":
+    if args.workload != "return_map":
+        import bench_workloads
+
+        bench_workloads.run(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

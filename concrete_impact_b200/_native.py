@@ -129,6 +129,36 @@ class RVEBatchC(ctypes.Structure):
     ]
 
 
+class RNOWindowC(ctypes.Structure):
+    """``cib_rno_window``."""
+
+    _fields_ = [
+        ("B", ctypes.c_int32),
+        ("T", ctypes.c_int32),
+        ("hidden", ctypes.c_int32),
+        ("loss_scale", ctypes.c_float),
+        ("ldt", ctypes.c_int64),
+        ("strain", ctypes.c_void_p),
+        ("rate", ctypes.c_void_p),
+        ("coef", ctypes.c_void_p),
+        ("target", ctypes.c_void_p),
+        ("z", ctypes.c_void_p),
+        ("W", ctypes.c_void_p * 4),
+        ("Wt", ctypes.c_void_p * 4),
+        ("bias", ctypes.c_void_p * 4),
+        ("skip", ctypes.c_void_p),
+        ("Z", ctypes.c_void_p * 3),
+        ("Xt", ctypes.c_void_p),
+        ("Ht", ctypes.c_void_p * 3),
+        ("stress", ctypes.c_void_p),
+        ("gS", ctypes.c_void_p),
+        ("loss_part", ctypes.c_void_p),
+        ("dYt", ctypes.c_void_p),
+        ("dZt", ctypes.c_void_p * 3),
+        ("err", ctypes.c_void_p),
+    ]
+
+
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
 _D = ctypes.c_double
@@ -158,6 +188,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_adam_step": (_I, [ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P] + [ctypes.c_float] * 4
                       + [_P, _P, ctypes.c_int32, _P, ctypes.c_int32, _P]),
     "cib_counter_increment": (_I, [_P, _P]),
+    "cib_rno_window_forward": (_I, [_P, _P]),
+    "cib_rno_window_backward": (_I, [_P, _P]),
     "cib_verlet_predict": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P]),
     "cib_verlet_correct": (_I, [_I64, _P, _D, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     "cib_rve_residual": (_I, [_P] * 9),

@@ -19,13 +19,13 @@
 #include <stdint.h>
 
 #include "cib_common.cuh"
+#include "umma.cuh"
 
 namespace cib {
 namespace {
 
 constexpr int GEMM_THREADS = 128;
 constexpr int KC = 64;  // K elements staged per chunk
-constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s
 
 enum Epi { EPI_F32 = 0, EPI_BIAS_F32 = 1, EPI_BIAS_GELU = 2, EPI_GELU_BWD = 3, EPI_PARTIAL = 4 };
 
@@ -49,52 +49,7 @@ struct GemmArgs {
   unsigned int* err;   // set to 1 when a wait times out
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// Byte offset of element (r, c) of a tile with KC columns in the canonical K-major layout.
-__device__ __forceinline__ uint32_t core_offset(int r, int c) {
-  return (uint32_t)((((r >> 3) * (KC / 8)) + (c >> 3)) * 128 + (r & 7) * 16 + (c & 7) * 2);
-}
-
-// Shared-memory matrix descriptor: start address, leading (K-direction core-matrix) byte
-// offset, stride (8-row group) byte offset, descriptor version 1, no swizzle.
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
-
-// Instruction descriptor: D f32, A and B bf16, both K-major, M = 128, N.
-__device__ __forceinline__ uint32_t idesc_bf16(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-}
-
-__device__ __forceinline__ uint64_t now_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  const uint64_t t0 = now_ns();
-  while (true) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (now_ns() - t0 > WAIT_LIMIT_NS) return false;
-  }
-}
-
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float x) {
-  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-  const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
-  return cdf + x * pdf;
-}
+using namespace umma;
 
 template <int EPI>
 __global__ void __launch_bounds__(GEMM_THREADS) umma_gemm_kernel(const GemmArgs a) {
@@ -132,13 +87,13 @@ __global__ void __launch_bounds__(GEMM_THREADS) umma_gemm_kernel(const GemmArgs 
       uint4 val = make_uint4(0, 0, 0, 0);
       if (m0 + r < a.M && k0 + c < k_end)
         val = *reinterpret_cast<const uint4*>(a.A + (size_t)(m0 + r) * a.lda + k0 + c);
-      *reinterpret_cast<uint4*>(sA + core_offset(r, c)) = val;
+      *reinterpret_cast<uint4*>(sA + core_offset(r, c, KC)) = val;
     }
     for (int v = tid; v < a.N * (KC / 8); v += GEMM_THREADS) {
       const int r = v / (KC / 8), c = (v % (KC / 8)) * 8;
       uint4 val = make_uint4(0, 0, 0, 0);
       if (k0 + c < k_end) val = *reinterpret_cast<const uint4*>(a.B + (size_t)r * a.ldb + k0 + c);
-      *reinterpret_cast<uint4*>(sB + core_offset(r, c)) = val;
+      *reinterpret_cast<uint4*>(sB + core_offset(r, c, KC)) = val;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();

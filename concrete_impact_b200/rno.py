@@ -128,6 +128,10 @@ class RNOSurrogate:
         self.step = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.learning_rate = float(config.learning_rate)
+        # fused window kernels (one CTA per 128 paths for the whole window) for width 128
+        self.fused = h == 128
+        self.skip: torch.Tensor | None = None  # 6x6 normalised elastic skip, fused path only
+        self._structs: dict = {}
         self._window: dict | None = None
         self._graph: torch.cuda.CUDAGraph | None = None
 
@@ -146,6 +150,8 @@ class RNOSurrogate:
             out[f"layers.{i}.weight"] = L.w.detach().cpu().clone()
             out[f"layers.{i}.bias"] = L.b.detach().cpu().clone()
         out["scales"] = torch.tensor([self.scales.strain, self.scales.rate, self.scales.stress], dtype=torch.float64)
+        if self.skip is not None:
+            out["skip"] = self.skip.detach().cpu().clone()
         return out
 
     def load_state_dict(self, state: dict[str, torch.Tensor]) -> None:
@@ -156,6 +162,9 @@ class RNOSurrogate:
             L.wt.copy_(L.w.T.to(torch.bfloat16))
         s = state["scales"].tolist()
         self.scales = RNOScales(*s)
+        self.skip = state["skip"].to(self.device).contiguous() if "skip" in state else None
+        self._structs = {}
+        self._graph = None
 
     # -- window buffers ---------------------------------------------------------------
     def _buffers(self, T: int, B: int) -> dict:
@@ -163,22 +172,23 @@ class RNOSurrogate:
             return self._window
         dev, h = self.device, self.config.hidden
         R = T * B
+        Rp = ((R + 63) // 64) * 64  # transposed buffers: K of the weight-gradient GEMMs, zero-padded
         f32, bf = torch.float32, torch.bfloat16
 
         def e(*shape, dtype=f32):
             return torch.zeros(shape, dtype=dtype, device=dev)
 
-        splits = max(1, min(64, R // 512))
+        splits = max(1, min(64, Rp // 512))
         self._window = {
-            "T": T, "B": B, "R": R, "splits": splits,
+            "T": T, "B": B, "R": R, "Rp": Rp, "splits": splits,
             "strain": e(T, B, 6), "rate": e(T, B, 6), "target": e(T, B, 6), "coef": e(T, B), "z": e(T + 1, B, 6),
-            "X": e(T, B, IN_PAD, dtype=bf), "Xt": e(IN_PAD, R, dtype=bf),
+            "X": e(T, B, IN_PAD, dtype=bf), "Xt": e(IN_PAD, Rp, dtype=bf),
             "Z": [e(T, B, h) for _ in range(3)], "H": [e(T, B, h, dtype=bf) for _ in range(3)],
-            "Ht": [e(h, R, dtype=bf) for _ in range(3)],
+            "Ht": [e(h, Rp, dtype=bf) for _ in range(3)],
             "Y": e(T, B, OUT_PAD), "gY": e(T, B, 6),
-            "loss_part": torch.zeros((T, (B + 255) // 256), dtype=torch.float64, device=dev),
-            "dY": e(B, OUT_PAD, dtype=bf), "dYt": e(OUT_PAD, R, dtype=bf),
-            "dZ": [e(B, h, dtype=bf) for _ in range(3)], "dZt": [e(h, R, dtype=bf) for _ in range(3)],
+            "loss_part": torch.zeros((T, (B + 127) // 128), dtype=torch.float64, device=dev),
+            "dY": e(B, OUT_PAD, dtype=bf), "dYt": e(OUT_PAD, Rp, dtype=bf),
+            "dZ": [e(B, h, dtype=bf) for _ in range(3)], "dZt": [e(h, Rp, dtype=bf) for _ in range(3)],
             "dX": e(B, IN_PAD), "dz": [e(B, 6), e(B, 6)],
             "partial": e(splits * h, h),
         }  # fmt: skip
@@ -186,7 +196,40 @@ class RNOSurrogate:
         return self._window
 
     # -- one window ---------------------------------------------------------------------
+    def _window_struct(self, w: dict, with_loss: bool) -> _native.RNOWindowC:
+        """C descriptor of a window's buffers (kept alive with the window)."""
+        key = (id(w), with_loss)
+        if key in self._structs:
+            return self._structs[key]
+        c = _native.RNOWindowC()
+        c.B, c.T, c.hidden = w["B"], w["T"], self.config.hidden
+        c.ldt = w["Rp"]
+        c.loss_scale = 1.0 / float(w["B"] * w["T"] * 6)
+        c.strain, c.rate, c.coef = w["strain"].data_ptr(), w["rate"].data_ptr(), w["coef"].data_ptr()
+        c.target = w["target"].data_ptr() if with_loss else None
+        c.z = w["z"].data_ptr()
+        for i, L in enumerate(self.layers):
+            c.W[i], c.Wt[i], c.bias[i] = L.wb.data_ptr(), L.wt.data_ptr(), L.b.data_ptr()
+        c.skip = None if self.skip is None else self.skip.data_ptr()
+        for i in range(3):
+            c.Z[i], c.Ht[i], c.dZt[i] = w["Z"][i].data_ptr(), w["Ht"][i].data_ptr(), w["dZt"][i].data_ptr()
+        c.Xt = w["Xt"].data_ptr()
+        c.stress = None
+        c.gS = w["gY"].data_ptr() if with_loss else None
+        c.loss_part = w["loss_part"].data_ptr() if with_loss else None
+        c.dYt = w["dYt"].data_ptr()
+        c.err = self.err.data_ptr()
+        self._structs = {k: v for k, v in self._structs.items() if k[0] == id(w)}
+        self._structs[key] = c
+        return c
+
     def _forward(self, w: dict, with_loss: bool) -> None:
+        if self.fused:
+            c = self._window_struct(w, with_loss)
+            _check(self.lib.cib_rno_window_forward(ctypes.byref(c), _native.stream_ptr()), "cib_rno_window_forward")
+            return
+        if self.skip is not None:
+            raise ValueError("the elastic skip term needs the fused kernels (hidden width 128)")
         T, B, R = w["T"], w["B"], w["R"]
         L = self.layers
         lib = self.lib
@@ -194,7 +237,7 @@ class RNOSurrogate:
         scale = 1.0 / float(B * T * 6)
         for t in range(T):
             _check(lib.cib_rno_input(B, w["strain"][t].data_ptr(), w["rate"][t].data_ptr(), w["z"][t].data_ptr(),
-                                     w["X"][t].data_ptr(), w["Xt"].data_ptr(), R, t * B, sp), "cib_rno_input")  # fmt: skip
+                                     w["X"][t].data_ptr(), w["Xt"].data_ptr(), w["Rp"], t * B, sp), "cib_rno_input")  # fmt: skip
             a = w["X"][t]
             for i in range(3):
                 gemm(EPI_BIAS_GELU, a, L[i].wb, bias=L[i].b, z=w["Z"][i][t], h=w["H"][i][t], ht=w["Ht"][i],
@@ -211,11 +254,23 @@ class RNOSurrogate:
         L = self.layers
         lib = self.lib
         sp = _native.stream_ptr()
+        if self.fused:
+            c = self._window_struct(w, True)
+            _check(lib.cib_rno_window_backward(ctypes.byref(c), sp), "cib_rno_window_backward")
+        else:
+            self._backward_steps(w)
+        self._weight_gradients(w)
+
+    def _backward_steps(self, w: dict) -> None:
+        T, B, R = w["T"], w["B"], w["R"]
+        L = self.layers
+        lib = self.lib
+        sp = _native.stream_ptr()
         dz_next, dz = w["dz"]
         dz_next.zero_()
         for t in range(T - 1, -1, -1):
             _check(lib.cib_rno_backward_head(B, w["gY"][t].data_ptr(), w["coef"][t].data_ptr(), dz_next.data_ptr(),
-                                             w["dY"].data_ptr(), w["dYt"].data_ptr(), R, t * B, sp),
+                                             w["dY"].data_ptr(), w["dYt"].data_ptr(), w["Rp"], t * B, sp),
                    "cib_rno_backward_head")  # fmt: skip
             grad = w["dY"]
             for i in (2, 1, 0):
@@ -226,7 +281,13 @@ class RNOSurrogate:
             _check(lib.cib_rno_backward_tail(B, dz_next.data_ptr(), w["dX"].data_ptr(), dz.data_ptr(), sp),
                    "cib_rno_backward_tail")  # fmt: skip
             dz_next, dz = dz, dz_next
-        # weight and bias gradients over all rows of the window (split-K GEMMs)
+
+    def _weight_gradients(self, w: dict) -> None:
+        """Weight and bias gradients over all rows of the window (split-K GEMMs)."""
+        R = w["R"]
+        L = self.layers
+        lib = self.lib
+        sp = _native.stream_ptr()
         h = self.config.hidden
         ins = [w["Xt"], w["Ht"][0], w["Ht"][1], w["Ht"][2]]
         outs = [w["dZt"][0], w["dZt"][1], w["dZt"][2], w["dYt"]]
@@ -236,7 +297,7 @@ class RNOSurrogate:
             part = w["partial"][: w["splits"] * m]
             gemm(EPI_PARTIAL, outs[i], ins[i], c=part, splits=w["splits"], err=self.err, rows=m)
             splitk_reduce(part.view(w["splits"], m, n) if n == h else part, w["splits"], m, n, L[i].gw)
-            _check(lib.cib_row_sum_bf16(m, R, outs[i].data_ptr(), R, L[i].gb.data_ptr(), sp), "cib_row_sum_bf16")
+            _check(lib.cib_row_sum_bf16(m, R, outs[i].data_ptr(), w["Rp"], L[i].gb.data_ptr(), sp), "cib_row_sum_bf16")
 
     def _adam(self) -> None:
         lib, sp, c = self.lib, _native.stream_ptr(), self.config
@@ -353,10 +414,50 @@ class RNOSurrogate:
         self._graph.replay()
 
     # -- inference ---------------------------------------------------------------------
+    def set_elastic_skip(self, stiffness) -> None:
+        """Add K (strain - z) to the stress output, K the given 6x6 stiffness (physical
+        units, e.g. the RVE's effective elastic tangent) in normalised units: the network then
+        learns the departure from the elastic response with the latent state in strain
+        units.  ``None`` removes it."""
+        if stiffness is None:
+            self.skip = None
+        else:
+            if not self.fused:
+                raise ValueError("the elastic skip term needs the fused kernels (hidden width 128)")
+            k = torch.as_tensor(np.asarray(stiffness, dtype=np.float64) * self.scales.strain / self.scales.stress,
+                                dtype=torch.float32)  # fmt: skip
+            self.skip = k.reshape(6, 6).contiguous().to(self.device)
+        self._structs = {}
+        self._graph = None
+
     def predict(self, strain: torch.Tensor, rate: torch.Tensor, z: torch.Tensor, coef: torch.Tensor,
                 buffers: dict | None = None) -> tuple[torch.Tensor, torch.Tensor, dict]:  # fmt: skip
         """One step for M points (physical strain (M, 6), rate (M, 6), latent (M, 6), coef
         (M,)): returns (stress (M, 6) in physical units, next latent (M, 6), buffers)."""
+        M = int(strain.shape[0])
+        if not self.fused:
+            return self._predict_unfused(strain, rate, z, coef, buffers)
+        dev = self.device
+        if buffers is None or buffers["M"] != M:
+            buffers = {"M": M, "z": torch.empty((2, M, 6), dtype=torch.float32, device=dev),
+                       "stress": torch.empty((1, M, 6), dtype=torch.float32, device=dev)}  # fmt: skip
+        s = self.scales
+        sn = (strain / s.strain).float().contiguous()
+        rn = (rate / s.rate).float().contiguous()
+        cf = coef.float().contiguous()
+        buffers["z"][0].copy_(z)
+        c = _native.RNOWindowC()
+        c.B, c.T, c.hidden = M, 1, self.config.hidden
+        c.strain, c.rate, c.coef, c.z = sn.data_ptr(), rn.data_ptr(), cf.data_ptr(), buffers["z"].data_ptr()
+        for i, L in enumerate(self.layers):
+            c.W[i], c.bias[i] = L.wb.data_ptr(), L.b.data_ptr()
+        c.skip = None if self.skip is None else self.skip.data_ptr()
+        c.stress = buffers["stress"].data_ptr()
+        c.err = self.err.data_ptr()
+        _check(self.lib.cib_rno_window_forward(ctypes.byref(c), _native.stream_ptr()), "cib_rno_window_forward")
+        return buffers["stress"][0] * s.stress, buffers["z"][1], buffers
+
+    def _predict_unfused(self, strain, rate, z, coef, buffers):
         M = int(strain.shape[0])
         dev, h = self.device, self.config.hidden
         if buffers is None or buffers["M"] != M:
@@ -388,6 +489,24 @@ class RNOSurrogate:
         """Stress predictions (P, T, 6) (physical units) along every path of ``data``."""
         P, T = data.paths, data.steps
         rates = data.rates()
+        if self.fused and P > 0:
+            s = self.scales
+            dev = self.device
+            sn = (data.strain[:, 1:] / s.strain).float().transpose(0, 1).contiguous()
+            rn = (rates / s.rate).float().transpose(0, 1).contiguous()
+            cf = (data.dt / self.config.tau_ref).float().transpose(0, 1).contiguous()
+            zs = torch.zeros((T + 1, P, 6), dtype=torch.float32, device=dev)
+            st = torch.empty((T, P, 6), dtype=torch.float32, device=dev)
+            c = _native.RNOWindowC()
+            c.B, c.T, c.hidden = P, T, self.config.hidden
+            c.strain, c.rate, c.coef, c.z = sn.data_ptr(), rn.data_ptr(), cf.data_ptr(), zs.data_ptr()
+            for i, L in enumerate(self.layers):
+                c.W[i], c.bias[i] = L.wb.data_ptr(), L.b.data_ptr()
+            c.skip = None if self.skip is None else self.skip.data_ptr()
+            c.stress = st.data_ptr()
+            c.err = self.err.data_ptr()
+            _check(self.lib.cib_rno_window_forward(ctypes.byref(c), _native.stream_ptr()), "cib_rno_window_forward")
+            return (st * s.stress).transpose(0, 1).contiguous()
         z = torch.zeros((P, 6), dtype=torch.float32, device=self.device)
         out = torch.empty((P, T, 6), dtype=torch.float32, device=self.device)
         buf = None

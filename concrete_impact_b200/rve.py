@@ -558,6 +558,7 @@ def solve_batch_step(
     diag: torch.Tensor | None = None,
     failure_context: Callable[[int, int], Exception] | None = None,
     live_mask: np.ndarray | None = None,
+    timers: dict | None = None,
 ) -> BatchStepResult:
     """Solve the microequilibrium of every RVE of the batch from its committed state.
 
@@ -565,6 +566,8 @@ def solve_batch_step(
     fluctuation.  On success the trial state of every RVE is its converged state (not yet
     committed).  ``live_mask`` restricts the solve to some RVEs; the others are left
     untouched and stay inactive (``batch.active``) for the response and tangent kernels.
+    ``timers``, when given, collects CUDA event pairs around the residual and PCG launches
+    (keys "residual", "pcg"; read them after a synchronize).
     """
     R = batch.nrve
     b = batch.batch_struct(update_settings)
@@ -581,7 +584,7 @@ def solve_batch_step(
     _set_active(batch, ~done)
     ns = newton
     for iteration in range(ns.max_iterations + 1):
-        batch.residual(b, batch.w, None, None)
+        _timed(timers, "residual", lambda: batch.residual(b, batch.w, None, None))
         rn2, wn2, fail = (t.cpu().numpy() for t in (batch.rnorm2, batch.wnorm2, batch.fail))
         live = ~done
         _raise_material_failure(batch, fail, live, failure_context)
@@ -600,8 +603,9 @@ def solve_batch_step(
             raise RVEEquilibriumError("maximum_iterations_exceeded", _failure_diag(batch, r, iteration, rnorm[r], tol[r],
                                                                                    last_inc[r], inc_tol[r]))  # fmt: skip
         _set_active(batch, live)
-        batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, R, batch.sys_rve, batch.sys_off,
-                  batch.pcg_status, batch.pcg_iters, batch.pcg_rel, batch.pcg_xnorm)  # fmt: skip
+        _timed(timers, "pcg", lambda: batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, R, batch.sys_rve,
+                                                batch.sys_off, batch.pcg_status, batch.pcg_iters, batch.pcg_rel,
+                                                batch.pcg_xnorm))  # fmt: skip
         status, piters, xnorm = (t.cpu().numpy() for t in (batch.pcg_status, batch.pcg_iters, batch.pcg_xnorm))
         pcg_total[live] += piters[live]
         bad = live & ((status == 2) | ~np.isfinite(xnorm))
@@ -630,6 +634,17 @@ def solve_batch_step(
     else:
         _set_active(batch, final_active)
     return BatchStepResult(iters_out, backtracks, res_out, tol_out, pcg_total)
+
+
+def _timed(timers: dict | None, key: str, fn) -> None:
+    if timers is None:
+        fn()
+        return
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    fn()
+    end.record()
+    timers.setdefault(key, []).append((start, end))
 
 
 def _set_active(batch: RVEBatch, mask: np.ndarray) -> None:

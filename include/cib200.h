@@ -363,7 +363,51 @@ int cib_adam_step(int32_t rows, int32_t cols, float* w, const float* g, float* m
                   void* stream);
 int cib_counter_increment(int32_t* counter, void* stream);
 
-/* --- Explicit macro dynamics (FE^2) ---------------------------------------------------
+/* --- Fused recurrent window (one CTA per 128 paths for all T steps) -------------------
+ * Forward over a window of T steps for B paths with hidden width 128, in normalised units:
+ * x = [strain, rate, z] (bf16), three bias+GELU layers, output layer Y (16);
+ * s = Y[0:6] + skip (strain - z) (skip: 6x6 row-major, NULL for none), z' = z + coef Y[6:12]
+ * (forward-Euler latent step, src/concrete_impact/nn/models/rve_rno.py:383-387).
+ * Layout: strain, rate, target, stress, gS (T, B, 6); coef (T, B); z (T + 1, B, 6) with
+ * z[0] read and z[1..T] written; W[l] bf16 row-major (out x in_pad) = 128x32, 128x128,
+ * 128x128, 16x128 and Wt[l] their transposes; bias[l] fp32; Z[l] (T, B, 128) fp32
+ * pre-activations; Xt (32, ldt), Ht[l] (128, ldt), dYt (16, ldt), dZt[l] (128, ldt) bf16
+ * transposes with column t B + p.  Optional outputs may be NULL in the forward (Z, Xt, Ht,
+ * stress, target/gS/loss_part); the backward needs Wt, Z, gS, dYt and dZt.
+ * loss_part (T, ceil(B / 128)): row 0 holds each CTA's sum of squared errors over the
+ * window, the other rows zero.  gS = loss_scale * 2 (s - target).  The backward runs the
+ * window in reverse with dz(T) = 0 and writes dY^T, dZ^T for the weight-gradient GEMMs.
+ * err (device uint32) becomes 1 when a tensor-core wait exceeds 2 s.  No reference
+ * counterpart (the reference runs torch.nn layers per step). */
+typedef struct cib_rno_window {
+  int32_t B;
+  int32_t T;
+  int32_t hidden;
+  float loss_scale;
+  int64_t ldt; /* leading dimension of Xt, Ht, dYt, dZt (>= T B; 0 means T B) */
+  const float* strain;
+  const float* rate;
+  const float* coef;
+  const float* target;
+  float* z;
+  const void* W[4];
+  const void* Wt[4];
+  const float* bias[4];
+  const float* skip;
+  float* Z[3];
+  void* Xt;
+  void* Ht[3];
+  float* stress;
+  float* gS;
+  double* loss_part;
+  void* dYt;
+  void* dZt[3];
+  unsigned int* err;
+} cib_rno_window;
+int cib_rno_window_forward(const cib_rno_window* w, void* stream);
+int cib_rno_window_backward(const cib_rno_window* w, void* stream);
+
+/* --- Explicit macro dynamics (FE^2)---------------------------------------------------
  * Velocity-Verlet step of src/fem/dynamics/material.py:164-219 with a lumped mass and
  * homogeneous Dirichlet DOFs (fixed[i] != 0): predictor u' = u + dt v + dt^2/2 a, then
  * corrector a' = (load_scale f_unit - f_int) / m, v' = v + dt/2 (a + a'). */

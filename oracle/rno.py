@@ -33,11 +33,13 @@ def gelu_grad(x):
     return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
 
 
-def window_forward_backward(params, strain, rate, target, coef, z0, bf16: bool = False):
+def window_forward_backward(params, strain, rate, target, coef, z0, bf16: bool = False, skip=None):
     """Loss and gradients of one window.
 
     params: list of (W (out, in_pad), b (out,)) for the 4 layers; strain/rate/target
-    (T, B, 6); coef (T, B); z0 (B, 6).  Returns (loss, grads [(dW, db)], z_T, Y (T, B, 16)).
+    (T, B, 6); coef (T, B); z0 (B, 6); skip: optional 6x6 K adding K (strain - z) to the
+    stress output.  Returns (loss, grads [(dW, db)], z_T, Y (T, B, 16)); Y[:, :, :6] is
+    the stress including the skip term.
     """
     rnd = bf16_round if bf16 else (lambda a: np.asarray(a, dtype=np.float64))
     T, B = strain.shape[0], strain.shape[1]
@@ -60,6 +62,9 @@ def window_forward_backward(params, strain, rate, target, coef, z0, bf16: bool =
             hl.append(h)
             a = h
         y = a @ Ws[3].T + bs[3]
+        if skip is not None:
+            y = y.copy()
+            y[:, :6] += (strain[t] - z[t]) @ np.asarray(skip, dtype=np.float64).T
         Zs.append(zl)
         Hs.append(hl)
         Y.append(y)
@@ -87,4 +92,6 @@ def window_forward_backward(params, strain, rate, target, coef, z0, bf16: bool =
             g = dzl
         dx = g @ Ws[0]
         dz_next = dz_next + dx[:, 12:18]
+        if skip is not None:
+            dz_next = dz_next - gY[t] @ np.asarray(skip, dtype=np.float64)
     return loss, grads, z[T], Y

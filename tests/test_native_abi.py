@@ -106,3 +106,36 @@ def test_material_validation_matches_reference_messages() -> None:
                                 ("rate_exponent", 0.5, "rate_exponent >= 1"), ("time_scale", 0.0, "time_scale > 0")]:  # fmt: skip
         with pytest.raises(ValueError, match=message):
             build_j2_viscoplastic_material({**base, key: value})
+
+
+def test_struct_layouts_match_c_header(tmp_path) -> None:
+    """sizeof/offsetof of the C structs (compiled from include/cib200.h with the host C
+    compiler) equal the ctypes mirrors' layouts."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    checks = {
+        "cib_rve_batch": (_native.RVEBatchC, ["nelem", "desc", "mats", "settings", "plastic_strain_n", "de"]),
+        "cib_rno_window": (_native.RNOWindowC, ["ldt", "strain", "W", "Wt", "bias", "skip", "Z", "Xt", "Ht", "stress",
+                                                "loss_part", "dYt", "dZt", "err"]),
+        "cib_phase_material": (_native.PhaseMaterialC, ["params"]),
+    }
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "cib200.h"', "int main(void) {"]
+    for name, (_, fields) in checks.items():
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for f in fields:
+            lines.append(f'  printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    include = Path(__file__).resolve().parent.parent / "include"
+    subprocess.run([cc, f"-I{include}", str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines())
+    for name, (cls, fields) in checks.items():
+        assert int(got[name]) == ctypes.sizeof(cls), name
+        for f in fields:
+            assert int(got[f"{name}.{f}"]) == getattr(cls, f).offset, f"{name}.{f}"

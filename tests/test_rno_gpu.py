@@ -34,9 +34,11 @@ def _rel(a, b) -> float:
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def test_window_gradients_match_oracle_and_autograd() -> None:
+@pytest.mark.parametrize("fused", [True, False])
+def test_window_gradients_match_oracle_and_autograd(fused: bool) -> None:
     T, B = 6, 256
     model = RNOSurrogate(RNOConfig(seed=3))
+    model.fused = fused
     strain, rate, target, coef, z0 = _window(T, B, 1)
     model.load_window(strain, rate, target, coef, z0)
     model.window_gradients(T, B)
@@ -68,6 +70,66 @@ def test_window_gradients_match_oracle_and_autograd() -> None:
     total.backward()
     for (gw, gb), W, b in zip(grads, Ws, bs):
         assert _rel(gw, W.grad.cpu().numpy()) < 5e-2 and _rel(gb, b.grad.cpu().numpy()) < 5e-2
+
+
+def test_fused_window_matches_unfused_kernels() -> None:
+    """The fused recurrent kernels and the per-step GEMM path compute the same window
+    (ragged batch: 300 paths = 2 full CTAs + 44 rows)."""
+    T, B = 7, 300
+    fused, plain = RNOSurrogate(RNOConfig(seed=4)), RNOSurrogate(RNOConfig(seed=4))
+    plain.fused = False
+    window = _window(T, B, 2)
+    for m in (fused, plain):
+        m.load_window(*window)
+        m.window_gradients(T, B)
+    torch.cuda.synchronize()
+    assert int(fused.err.item()) == 0 and int(plain.err.item()) == 0
+    assert fused.window_loss() == pytest.approx(plain.window_loss(), rel=1e-5)
+    wf, wp = fused._window, plain._window
+    assert _rel(wf["z"].cpu(), wp["z"].cpu()) < 1e-5
+    for i in range(3):
+        assert _rel(wf["Z"][i].cpu(), wp["Z"][i].cpu()) < 1e-5
+        assert _rel(wf["Ht"][i].float().cpu(), wp["Ht"][i].float().cpu()) < 1e-3
+        assert _rel(wf["dZt"][i].float().cpu(), wp["dZt"][i].float().cpu()) < 1e-2
+    for (gf, bf), (gp, bp) in zip(fused.gradients(), plain.gradients()):
+        assert _rel(gf.cpu(), gp.cpu()) < 1e-2 and _rel(bf.cpu(), bp.cpu()) < 1e-2
+
+
+def test_fused_skip_gradients_match_oracle() -> None:
+    T, B = 5, 200
+    model = RNOSurrogate(RNOConfig(seed=6), RNOScales(1.0, 1.0, 1.0))
+    g = np.random.default_rng(3)
+    K = g.normal(size=(6, 6)) * 0.3
+    model.set_elastic_skip(K)  # unit scales: the normalised skip is K itself
+    window = _window(T, B, 5)
+    model.load_window(*window)
+    model.window_gradients(T, B)
+    torch.cuda.synchronize()
+    assert int(model.err.item()) == 0
+    grads = [(gw.cpu().numpy(), gb.cpu().numpy()) for gw, gb in model.gradients()]
+    params = [(L.w.cpu().numpy(), L.b.cpu().numpy()) for L in model.layers]
+    np_in = [x.cpu().numpy().astype(np.float64) for x in window]
+    skip32 = model.skip.cpu().numpy().astype(np.float64)
+    oloss, ograds, oz, _ = window_forward_backward(params, *np_in, bf16=True, skip=skip32)
+    assert model.window_loss() == pytest.approx(oloss, rel=1e-3)
+    assert _rel(model._window["z"][T].cpu().numpy(), oz) < 1e-3
+    for (gw, gb), (ow, ob) in zip(grads, ograds):
+        assert _rel(gw, ow) < 2e-2 and _rel(gb, ob) < 2e-2
+
+
+def test_fused_predict_and_rollout_match_unfused() -> None:
+    data = _material_point_dataset(P=130, T=12, seed=11)
+    rates = data.rates()
+    scales = RNOScales.from_data(data.strain[:, 1:], rates, data.stress[:, 1:])
+    fused, plain = RNOSurrogate(RNOConfig(seed=2), scales), RNOSurrogate(RNOConfig(seed=2), scales)
+    plain.fused = False
+    z = torch.randn((130, 6), device="cuda") * 0.1
+    coef = torch.rand(130, device="cuda") * 0.2
+    sf, zf, _ = fused.predict(data.strain[:, 3], rates[:, 2], z, coef)
+    sp, zp, _ = plain.predict(data.strain[:, 3], rates[:, 2], z, coef)
+    assert _rel(sf.cpu(), sp.cpu()) < 1e-5 and _rel(zf.cpu(), zp.cpu()) < 1e-5
+    rf, rp = fused.rollout(data), plain.rollout(data)
+    assert _rel(rf.cpu(), rp.cpu()) < 1e-4
 
 
 def _material_point_dataset(P: int, T: int, seed: int, dt: float = 2.0e-6) -> RNODataset:
