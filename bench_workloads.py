@@ -1,4 +1,4 @@
-"""The RVE workloads of ``bench.py --workload rve_path|rve_batch`` (one JSON line on rank 0).
+"""The workloads of ``bench.py --workload rve_path|rve_batch|rno_train|fe2`` (one JSON line on rank 0).
 
 * rve_path  -- one 8^3 two-phase concrete RVE, mixed-control uniaxial compression to
   -0.5 % in 100 steps at 10 /s (free components at zero macro stress), FP64.  Metric:
@@ -8,6 +8,11 @@
   macro strain path; one batched Newton solve per time index, FP32 element kernels and
   FP64 reductions.  Metric: micro Gauss-point return-map evaluations per second inside
   the Newton solves (all residual passes of all RVEs), with accepted RVE steps/s beside it.
+* rno_train -- 2000 RVE paths x 200 steps generated by the batched solver, then surrogate
+  training; metric: training path-steps/s, with the held-out FP64 error beside it.
+* fe2       -- the 64x16x16 impact bar with surrogate macro points behind the error gate;
+  metric: macro steps/s, with all-direct FE^2 timed beside it and the surrogate's error
+  against all-direct FP64 FE^2 on a 64x2x2 bar.
 
 The CPU baseline of both is the NumPy/SciPy oracle of the reference's RVE solve (direct
 sparse solves, the reference's algorithm) timed on the host on a bounded sample.
@@ -204,6 +209,109 @@ def run_rve_batch(args: argparse.Namespace) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------
+# rno_train
+
+
+def _tensor_peak() -> tuple[float, str]:
+    from pathlib import Path
+
+    path = Path(__file__).resolve().parent / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return float(json.loads(path.read_text())["bf16_tflops"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 1590.0, "fallback"
+
+
+def run_rno_train(args: argparse.Namespace) -> None:
+    import torch
+
+    from bench import ClockSampler
+    from concrete_impact_b200.benchmarks import rno_training_workload
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    with ClockSampler(local) as clocks:
+        out = rno_training_workload(epochs=args.steps, warmup_epochs=args.warmup)
+    if rank != 0:
+        return
+    seconds = out["train_ms"] / 1e3
+    value = out["path_steps"] / seconds
+    peak, kind = _tensor_peak()
+    achieved = out["flop"] / seconds / 1e12
+    line = _line(args, "surrogate training throughput (path-steps/s; BF16 tcgen05 forward+backward, TBPTT 50, "
+                       "batch 512, Adam)", value, "path-steps/s",
+                 "rno_train: 2000 RVE paths x 200 steps (8^3 concrete RVE, FP32 solver), MLP 18-128-128-128-12 GELU",
+                 {"ms_per_step": out["train_ms"] / max(out["epochs"], 1),
+                  "dtype": "bf16 weights/activations, fp32 accumulation",
+                  "epochs_timed": out["epochs"], "windows_timed": out["windows"],
+                  "data_generation_s": out["data_generation_s"],
+                  "val_error": {"trained": out["error_trained"], "untrained": out["error_untrained"],
+                                "elastic_predictor": out["error_elastic"],
+                                "note": "relative Frobenius stress error on 256 held-out paths solved in FP64"},
+                  "loss_first_last": [out["loss_first"], out["loss_last"]],
+                  "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                               "frac": achieved / peak, "traffic": None, "peak_kind": f"{kind} (cuBLAS bf16, burst)",
+                               "kernel": "rno_window_forward/backward + split-K weight-gradient GEMMs",
+                               "note": "219,648 FLOP per path-step; the time recursion leaves B/128 CTAs per step"},
+                  "gpu_launches": None,
+                  "e2e": {"value": value, "unit": "path-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
+                          "path": "device-resident dataset; one loss read-back per epoch"},
+                  "clocks": clocks.summary(), "cpu_baseline": None})  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# fe2
+
+
+def run_fe2(args: argparse.Namespace) -> None:
+    """Train the surrogate (random + impact calibration paths), check it against all-direct
+    FE^2 (FP64 RVEs) on a 64x2x2 bar, then time surrogate FE^2 on the 64x16x16 bar for
+    ``--steps`` macro steps and all-direct FE^2 (FP32 RVEs) on the same bar for a short
+    window from rest.  CIB_FE2_RECIPE (JSON of FE2Recipe fields), CIB_FE2_ACCURACY_STEPS and
+    CIB_FE2_DIRECT_STEPS override the defaults."""
+    import torch
+
+    from bench import ClockSampler
+    from concrete_impact_b200.benchmarks import FE2Recipe, fe2_accuracy, fe2_speed, train_fe2_surrogate
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    fields = json.loads(os.environ.get("CIB_FE2_RECIPE", "{}"))
+    recipe = FE2Recipe(**{k: tuple(v) if isinstance(v, list) else v for k, v in fields.items()})
+    rno, envelope, info = train_fe2_surrogate(recipe)
+    acc = fe2_accuracy(rno, envelope, steps=int(os.environ.get("CIB_FE2_ACCURACY_STEPS", "300")))
+    with ClockSampler(local) as clocks:
+        speed = fe2_speed(rno, envelope, rno_steps=args.steps, rno_warmup=args.warmup,
+                          direct_steps=int(os.environ.get("CIB_FE2_DIRECT_STEPS", "3")))  # fmt: skip
+    if rank != 0:
+        return
+    value = speed["rno_steps_per_s"]
+    direct = speed.get("direct_steps_per_s")
+    line = _line(args, "FE2 macro steps/s with surrogate macro points (64x16x16 Hex8 bar, 131,072 macro GP, "
+                       "8^3 RVE fallback)", value, "macro steps/s",
+                 "fe2: velocity-Verlet bar 0.64x0.16x0.16 m, half-sine 50 MPa 50 us, rho 2400, CFL 0.5",
+                 {"ms_per_step": speed["rno_ms"] / speed["rno_steps"], "dtype": "bf16 surrogate, f64 macro fields",
+                  "direct_steps_per_s": direct, "speedup_vs_direct": value / direct if direct else None,
+                  "direct_ms_per_step": speed.get("direct_ms"), "accuracy": acc,
+                  "training": {**info, "recipe": recipe.__dict__, "envelope": envelope},
+                  "gate": {"flagged_points": speed["flagged_points"], "fallback_steps": speed["fallback_steps"]},
+                  "simulated_time_s": speed["simulated_time_s"],
+                  "roofline": {"bound": "tensor", "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
+                               "traffic": None, "note": "per step: one fused surrogate launch (T = 1, 1,024 CTAs) "
+                                                        "plus the macro Hex8 and Verlet kernels"},
+                  "gpu_launches": None,
+                  "e2e": {"value": value, "unit": "macro steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                          "path": "ExplicitFE2.run on device-resident macro fields"},
+                  "clocks": clocks.summary(), "cpu_baseline": None})  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args: argparse.Namespace) -> None:
     """``--impl reference``: the oracle alone on the workload's CPU sample (rank 0)."""
     if int(os.environ.get("RANK", "0")) != 0:
@@ -265,5 +373,9 @@ def run(args: argparse.Namespace) -> None:
         run_rve_path(args)
     elif args.workload == "rve_batch":
         run_rve_batch(args)
+    elif args.workload == "rno_train":
+        run_rno_train(args)
+    elif args.workload == "fe2":
+        run_fe2(args)
     else:
         raise SystemExit(f"unknown workload {args.workload}")

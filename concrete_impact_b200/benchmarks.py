@@ -10,6 +10,13 @@ rve_heterogeneous.py, dynamic_viscoplastic.py) for the concrete RVE of this pack
   own random piecewise-linear macro strain path (4 segments, |strain| <= 1 %, strain rate
   log-uniform in 1..1000 /s, 200 steps), all advanced by one batched Newton solve per
   time index with FP32 element kernels and FP64 reductions.
+* ``rno_training_workload`` -- 2000 RVE paths x 200 steps from the batched solver, then
+  surrogate training (MLP 18-128-128-128-12, BF16, batch 512 paths, TBPTT 50, Adam) scored
+  on held-out paths solved in FP64.
+* ``train_fe2_surrogate`` / ``fe2_accuracy`` / ``fe2_speed`` -- the explicit impact bar
+  (64 x 16 x 16 Hex8, 0.01 m elements, half-sine 50 MPa over 50 us, density 2400) with the
+  surrogate at every macro point behind the error gate, checked against all-direct FE^2
+  and timed against it.
 
 Each returns a dict of measured quantities; ``bench.py --workload`` prints them as its
 JSON line.  Timing uses CUDA events around whole steps on the current stream.
@@ -163,3 +170,173 @@ def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision:
             "stress_last": stress_h.numpy().copy(), "kernel_ms": kernel_ms, "kernel_launches": launches,
             "plastic_fraction": plastic, "h2d_bytes_per_step": int(batch.nrve * 7 * 8),
             "d2h_bytes_per_step": int(batch.nrve * 6 * 8), **counts}  # fmt: skip
+
+
+# ---------------------------------------------------------------------------------------
+# Surrogate training on RVE paths.
+
+RNO_FORWARD_FLOP = 2 * (18 * 128 + 128 * 128 * 2 + 128 * 12)  # 73,216 per path-step (unpadded)
+RNO_TRAIN_FLOP = 3 * RNO_FORWARD_FLOP  # forward + input-gradient + weight-gradient products
+
+
+def effective_elastic_tangent(model: StructuredHex8RVE) -> np.ndarray:
+    """The RVE's homogenised elastic stiffness: the effective tangent of one FP64 solve at a
+    strain far below yield (solve_rve_microequilibrium with the tangent requested)."""
+    from .materials import MaterialResponseRequirements
+    from .rve import RVERequest
+
+    cache = build_rve_operator_cache(model)
+    req = RVERequest(np.full(6, 1.0e-9), 1.0e-6, UPDATE_SETTINGS, MaterialResponseRequirements(tangent=True))
+    return np.asarray(solve_rve_microequilibrium(model, req, initialize_rve_state(model), cache).effective_tangent)
+
+
+def rno_training_workload(paths: int = 2000, steps: int = 200, epochs: int = 300, warmup_epochs: int = 1,
+                          val_paths: int = 256, config=None) -> dict:  # fmt: skip
+    """Generate ``paths`` RVE paths (8^3 concrete RVE, FP32 solver), train the surrogate
+    (batch 512 paths, TBPTT 50, Adam) for ``warmup_epochs`` + ``epochs`` epochs, timing the
+    latter, and score it on ``val_paths`` held-out paths solved in FP64."""
+    from .rno import RNOConfig, RNOScales, RNOSurrogate
+    from .rno_data import PathSetSpec, generate_rve_paths, relative_stress_error
+
+    out: dict = {}
+    model32, model64 = concrete_rve(8, 0, 32), concrete_rve(8, 0, 64)
+    t0 = time.perf_counter()
+    data = generate_rve_paths(model32, PathSetSpec(paths, steps, seed=20000), UPDATE_SETTINGS, precision=32)
+    torch.cuda.synchronize()
+    out["data_generation_s"] = time.perf_counter() - t0
+    val = generate_rve_paths(model64, PathSetSpec(val_paths, steps, seed=30000), UPDATE_SETTINGS, precision=64)
+    scales = RNOScales.from_data(data.strain[:, 1:], data.rates(), data.stress[:, 1:])
+    rno = RNOSurrogate(config or RNOConfig(), scales)
+    c_eff = torch.as_tensor(effective_elastic_tangent(model64), device=val.strain.device)
+    target = val.stress[:, 1:]
+    out["error_untrained"] = relative_stress_error(rno.rollout(val), target)
+    out["error_elastic"] = relative_stress_error(val.strain[:, 1:] @ c_eff.T, target)
+    history = rno.fit(data, warmup_epochs)
+    c = rno.config
+    batch = min(c.batch_paths, paths)
+    batches = paths // batch
+    ms = _elapsed_ms(lambda: history.extend(rno.fit(data, epochs)))
+    path_steps = epochs * batches * batch * steps
+    out.update({"train_ms": ms, "path_steps": path_steps, "epochs": epochs,
+                "windows": epochs * batches * (steps // c.tbptt_steps), "loss_first": history[0],
+                "loss_last": history[-1], "error_trained": relative_stress_error(rno.rollout(val), target),
+                "flop": path_steps * RNO_TRAIN_FLOP, "model": rno})  # fmt: skip
+    return out
+
+
+# ---------------------------------------------------------------------------------------
+# FE^2 explicit impact: surrogate-driven vs direct RVE macro points.
+
+
+@dataclass(frozen=True)
+class FE2Recipe:
+    """How the deployed surrogate is trained: random RVE paths plus impact paths taken from
+    direct FE^2 runs of a calibration bar at other pulse amplitudes (the reference's
+    impact_path data source)."""
+
+    random_paths: int = 2000
+    path_steps: int = 200
+    impact_amplitudes: tuple[float, ...] = (30.0e6, 70.0e6)
+    calibration_divisions: tuple[int, int, int] = (32, 2, 2)
+    epochs: int = 400
+    tau_ref: float = 1.0e-3
+    learning_rate: float = 1.0e-3
+    final_lr_fraction: float = 0.02
+
+
+def train_fe2_surrogate(recipe: FE2Recipe, log=None):
+    """Data generation and training for the FE^2 surrogate; returns (rno, envelope, info)."""
+    import math
+
+    from .rno import RNOConfig, RNOScales, RNOSurrogate
+    from .rno_data import PathSetSpec, concat_datasets, generate_rve_paths, impact_paths, input_envelope
+
+    model32 = concrete_rve(8, 0, 32)
+    info: dict = {}
+    t0 = time.perf_counter()
+    sets = []
+    if recipe.random_paths:
+        sets.append(generate_rve_paths(model32, PathSetSpec(recipe.random_paths, recipe.path_steps, seed=20000),
+                                       UPDATE_SETTINGS, precision=32))  # fmt: skip
+    if recipe.impact_amplitudes:
+        lengths = tuple(0.01 * d for d in recipe.calibration_divisions)
+        sets.append(impact_paths(model32, recipe.impact_amplitudes, recipe.path_steps, UPDATE_SETTINGS,
+                                 divisions=recipe.calibration_divisions, lengths=lengths, precision=32))  # fmt: skip
+    data = concat_datasets(*sets)
+    torch.cuda.synchronize()
+    info["data_generation_s"] = time.perf_counter() - t0
+    info["training_paths"] = data.paths
+    scales = RNOScales.from_data(data.strain[:, 1:], data.rates(), data.stress[:, 1:])
+    rno = RNOSurrogate(RNOConfig(tau_ref=recipe.tau_ref, learning_rate=recipe.learning_rate), scales)
+    lr0, frac, E = recipe.learning_rate, recipe.final_lr_fraction, recipe.epochs
+    schedule = lambda e: lr0 * (frac + (1.0 - frac) * 0.5 * (1.0 + math.cos(math.pi * e / max(E, 1))))  # noqa: E731
+    t0 = time.perf_counter()
+    history = rno.fit(data, E, lr_schedule=schedule, log=log)
+    torch.cuda.synchronize()
+    info["training_s"] = time.perf_counter() - t0
+    info["loss_first_last"] = [history[0], history[-1]] if history else None
+    return rno, input_envelope(scales, data), info
+
+
+def _record_run(fe2, steps: int) -> tuple[torch.Tensor, torch.Tensor]:
+    """Run ``steps`` steps; (stress (steps, P, 6), displacement (steps, 3N)) at every step."""
+    stress = torch.empty((steps, fe2.bar.points, 6), dtype=torch.float64, device=fe2.u.device)
+    disp = torch.empty((steps, fe2.u.numel()), dtype=torch.float64, device=fe2.u.device)
+    for t in range(steps):
+        fe2.step()
+        stress[t] = fe2.last_stress
+        disp[t] = fe2.u
+    return stress, disp
+
+
+def fe2_accuracy(rno, envelope, steps: int = 300, divisions=(64, 2, 2), precision_direct: int = 64,
+                 fallback_capacity: int = 512) -> dict:  # fmt: skip
+    """Surrogate FE^2 (with the error gate and direct fallback) against all-direct FE^2 on
+    the same bar (0.01 m elements, half-sine 50 MPa, 50 us): relative Frobenius errors of
+    the macro stress and displacement histories."""
+    from .fe2 import DirectRVEPoints, ExplicitFE2, RNOPoints, build_macro_bar, stable_time_step
+    from .rno_data import relative_stress_error
+
+    model_ref = concrete_rve(8, 0, precision_direct)
+    lengths = tuple(0.01 * d for d in divisions)
+    bar = build_macro_bar(divisions, lengths, 2400.0)
+    dt = stable_time_step(bar, model_ref.material.maximum_wave_speed, 0.5)
+    direct = ExplicitFE2(bar, DirectRVEPoints(model_ref, bar.points, UPDATE_SETTINGS, precision=precision_direct), dt)
+    s_ref, u_ref = _record_run(direct, steps)
+    del direct
+    gate = RNOPoints(rno, bar.points, envelope, concrete_rve(8, 0, 32), UPDATE_SETTINGS, fallback_capacity=fallback_capacity)
+    surrogate = ExplicitFE2(bar, gate, dt)
+    s_rno, u_rno = _record_run(surrogate, steps)
+    return {"steps": steps, "divisions": list(divisions), "dt": dt, "points": bar.points,
+            "stress_error": relative_stress_error(s_rno, s_ref), "displacement_error": relative_stress_error(u_rno, u_ref),
+            "flagged_points": int(gate.slots_used), "fallback_steps": int(gate.fallback_steps),
+            "stress_rms_pa": float(s_ref.pow(2).mean().sqrt().item())}  # fmt: skip
+
+
+def fe2_speed(rno, envelope, rno_steps: int = 5000, rno_warmup: int = 5, direct_steps: int = 3,
+              divisions=(64, 16, 16)) -> dict:  # fmt: skip
+    """Macro steps/s of surrogate FE^2 (``rno_steps`` steps) and of all-direct FE^2 (FP32 RVEs,
+    ``direct_steps`` steps from rest) on the full bar, CUDA-event timed."""
+    from .fe2 import DirectRVEPoints, ExplicitFE2, RNOPoints, build_macro_bar, stable_time_step
+
+    model32 = concrete_rve(8, 0, 32)
+    lengths = tuple(0.01 * d for d in divisions)
+    bar = build_macro_bar(divisions, lengths, 2400.0)
+    dt = stable_time_step(bar, model32.material.maximum_wave_speed, 0.5)
+    gate = RNOPoints(rno, bar.points, envelope, model32, UPDATE_SETTINGS, fallback_capacity=2048)
+    fe2 = ExplicitFE2(bar, gate, dt)
+    fe2.run(rno_warmup)
+    rno_ms = _elapsed_ms(lambda: fe2.run(rno_steps))
+    out = {"points": bar.points, "dt": dt, "rno_steps": rno_steps, "rno_ms": rno_ms,
+           "rno_steps_per_s": rno_steps / (rno_ms / 1e3), "flagged_points": int(gate.slots_used),
+           "fallback_steps": int(gate.fallback_steps), "simulated_time_s": (rno_warmup + rno_steps) * dt}  # fmt: skip
+    del fe2, gate
+    torch.cuda.empty_cache()
+    if direct_steps > 0:
+        direct = ExplicitFE2(bar, DirectRVEPoints(model32, bar.points, UPDATE_SETTINGS, precision=32), dt)
+        per_step = [_elapsed_ms(direct.step) for _ in range(direct_steps)]
+        out.update({"direct_steps": direct_steps, "direct_ms": per_step,
+                    "direct_steps_per_s": direct_steps / (sum(per_step) / 1e3)})  # fmt: skip
+        del direct
+        torch.cuda.empty_cache()
+    return out

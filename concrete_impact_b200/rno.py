@@ -375,7 +375,8 @@ class RNOSurrogate:
             if lr_schedule is not None:
                 self.set_learning_rate(lr_schedule(epoch))
             perm = torch.randperm(P, generator=gen)
-            losses = []
+            loss_sum = torch.zeros((), dtype=torch.float64, device=self.device)
+            windows = 0
             for start in range(0, P - B + 1, B):
                 idx = perm[start : start + B].to(self.device)
                 z0 = torch.zeros((B, 6), dtype=torch.float32, device=self.device)
@@ -387,9 +388,10 @@ class RNOSurrogate:
                         self._replay(W, B)
                     else:
                         self.window_step(W, B)
-                    losses.append(self.window_loss())
+                    loss_sum += self._window["loss_part"].sum()  # stays on the device
+                    windows += 1
                     z0 = self._window["z"][W].clone()
-            history.append(float(np.mean(losses)))
+            history.append(float(loss_sum.item()) / float(windows * B * W * 6))
             if log is not None:
                 log(epoch, history[-1])
         if int(self.err.item()) != 0:
