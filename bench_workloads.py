@@ -268,6 +268,14 @@ def run_rno_train(args: argparse.Namespace) -> None:
 # fe2
 
 
+def _progress(stage: str, seconds: float, payload: dict) -> None:
+    """Intermediate results on stderr, so that a run that stops later still reports them."""
+    import sys
+
+    sys.stderr.write(json.dumps({"stage": stage, "elapsed_s": seconds, **payload}, default=str) + "\n")
+    sys.stderr.flush()
+
+
 def run_fe2(args: argparse.Namespace) -> None:
     """Train the surrogate (random + impact calibration paths), check it against all-direct
     FE^2 (FP64 RVEs) on a 64x2x2 bar, then time surrogate FE^2 on the 64x16x16 bar for
@@ -284,8 +292,11 @@ def run_fe2(args: argparse.Namespace) -> None:
     torch.cuda.set_device(local)
     fields = json.loads(os.environ.get("CIB_FE2_RECIPE", "{}"))
     recipe = FE2Recipe(**{k: tuple(v) if isinstance(v, list) else v for k, v in fields.items()})
+    t0 = time.perf_counter()
     rno, envelope, info = train_fe2_surrogate(recipe)
-    acc = fe2_accuracy(rno, envelope, steps=int(os.environ.get("CIB_FE2_ACCURACY_STEPS", "300")))
+    _progress("trained", time.perf_counter() - t0, info)
+    acc = fe2_accuracy(rno, envelope, steps=int(os.environ.get("CIB_FE2_ACCURACY_STEPS", "400")))
+    _progress("accuracy", time.perf_counter() - t0, acc)
     with ClockSampler(local) as clocks:
         speed = fe2_speed(rno, envelope, rno_steps=args.steps, rno_warmup=args.warmup,
                           direct_steps=int(os.environ.get("CIB_FE2_DIRECT_STEPS", "3")))  # fmt: skip
@@ -296,7 +307,7 @@ def run_fe2(args: argparse.Namespace) -> None:
     line = _line(args, "FE2 macro steps/s with surrogate macro points (64x16x16 Hex8 bar, 131,072 macro GP, "
                        "8^3 RVE fallback)", value, "macro steps/s",
                  "fe2: velocity-Verlet bar 0.64x0.16x0.16 m, half-sine 50 MPa 50 us, rho 2400, CFL 0.5",
-                 {"ms_per_step": speed["rno_ms"] / speed["rno_steps"], "dtype": "bf16 surrogate, f64 macro fields",
+                 {"ms_per_step": speed["rno_ms"] / max(speed["rno_steps"], 1), "dtype": "bf16 surrogate, f64 macro fields",
                   "direct_steps_per_s": direct, "speedup_vs_direct": value / direct if direct else None,
                   "direct_ms_per_step": speed.get("direct_ms"), "accuracy": acc,
                   "training": {**info, "recipe": recipe.__dict__, "envelope": envelope},

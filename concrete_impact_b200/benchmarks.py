@@ -234,12 +234,13 @@ class FE2Recipe:
     direct FE^2 runs of a calibration bar at other pulse amplitudes (the reference's
     impact_path data source)."""
 
-    random_paths: int = 2000
-    path_steps: int = 200
-    impact_amplitudes: tuple[float, ...] = (30.0e6, 70.0e6)
-    calibration_divisions: tuple[int, int, int] = (32, 2, 2)
-    epochs: int = 400
-    tau_ref: float = 1.0e-3
+    random_paths: int = 0
+    path_steps: int = 400
+    impact_amplitudes: tuple[float, ...] = (20.0e6, 30.0e6, 40.0e6, 60.0e6, 70.0e6, 80.0e6)
+    calibration_divisions: tuple[int, int, int] = (64, 2, 2)
+    point_stride: int = 4
+    epochs: int = 1000
+    tau_ref: float = 1.0e-5
     learning_rate: float = 1.0e-3
     final_lr_fraction: float = 0.02
 
@@ -261,7 +262,8 @@ def train_fe2_surrogate(recipe: FE2Recipe, log=None):
     if recipe.impact_amplitudes:
         lengths = tuple(0.01 * d for d in recipe.calibration_divisions)
         sets.append(impact_paths(model32, recipe.impact_amplitudes, recipe.path_steps, UPDATE_SETTINGS,
-                                 divisions=recipe.calibration_divisions, lengths=lengths, precision=32))  # fmt: skip
+                                 divisions=recipe.calibration_divisions, lengths=lengths, precision=32,
+                                 point_stride=recipe.point_stride))  # fmt: skip
     data = concat_datasets(*sets)
     torch.cuda.synchronize()
     info["data_generation_s"] = time.perf_counter() - t0
@@ -289,8 +291,8 @@ def _record_run(fe2, steps: int) -> tuple[torch.Tensor, torch.Tensor]:
     return stress, disp
 
 
-def fe2_accuracy(rno, envelope, steps: int = 300, divisions=(64, 2, 2), precision_direct: int = 64,
-                 fallback_capacity: int = 512) -> dict:  # fmt: skip
+def fe2_accuracy(rno, envelope, steps: int = 400, divisions=(64, 2, 2), precision_direct: int = 64,
+                 fallback_capacity: int | None = None) -> dict:  # fmt: skip
     """Surrogate FE^2 (with the error gate and direct fallback) against all-direct FE^2 on
     the same bar (0.01 m elements, half-sine 50 MPa, 50 us): relative Frobenius errors of
     the macro stress and displacement histories."""
@@ -304,7 +306,8 @@ def fe2_accuracy(rno, envelope, steps: int = 300, divisions=(64, 2, 2), precisio
     direct = ExplicitFE2(bar, DirectRVEPoints(model_ref, bar.points, UPDATE_SETTINGS, precision=precision_direct), dt)
     s_ref, u_ref = _record_run(direct, steps)
     del direct
-    gate = RNOPoints(rno, bar.points, envelope, concrete_rve(8, 0, 32), UPDATE_SETTINGS, fallback_capacity=fallback_capacity)
+    gate = RNOPoints(rno, bar.points, envelope, concrete_rve(8, 0, 32), UPDATE_SETTINGS,
+                     fallback_capacity=fallback_capacity or bar.points)  # fmt: skip
     surrogate = ExplicitFE2(bar, gate, dt)
     s_rno, u_rno = _record_run(surrogate, steps)
     return {"steps": steps, "divisions": list(divisions), "dt": dt, "points": bar.points,
@@ -314,7 +317,7 @@ def fe2_accuracy(rno, envelope, steps: int = 300, divisions=(64, 2, 2), precisio
 
 
 def fe2_speed(rno, envelope, rno_steps: int = 5000, rno_warmup: int = 5, direct_steps: int = 3,
-              divisions=(64, 16, 16)) -> dict:  # fmt: skip
+              divisions=(64, 16, 16), fallback_capacity: int = 32768, time_limit_s: float = 180.0) -> dict:  # fmt: skip
     """Macro steps/s of surrogate FE^2 (``rno_steps`` steps) and of all-direct FE^2 (FP32 RVEs,
     ``direct_steps`` steps from rest) on the full bar, CUDA-event timed."""
     from .fe2 import DirectRVEPoints, ExplicitFE2, RNOPoints, build_macro_bar, stable_time_step
@@ -323,13 +326,28 @@ def fe2_speed(rno, envelope, rno_steps: int = 5000, rno_warmup: int = 5, direct_
     lengths = tuple(0.01 * d for d in divisions)
     bar = build_macro_bar(divisions, lengths, 2400.0)
     dt = stable_time_step(bar, model32.material.maximum_wave_speed, 0.5)
-    gate = RNOPoints(rno, bar.points, envelope, model32, UPDATE_SETTINGS, fallback_capacity=2048)
+    gate = RNOPoints(rno, bar.points, envelope, model32, UPDATE_SETTINGS, fallback_capacity=fallback_capacity)
     fe2 = ExplicitFE2(bar, gate, dt)
     fe2.run(rno_warmup)
-    rno_ms = _elapsed_ms(lambda: fe2.run(rno_steps))
-    out = {"points": bar.points, "dt": dt, "rno_steps": rno_steps, "rno_ms": rno_ms,
-           "rno_steps_per_s": rno_steps / (rno_ms / 1e3), "flagged_points": int(gate.slots_used),
-           "fallback_steps": int(gate.fallback_steps), "simulated_time_s": (rno_warmup + rno_steps) * dt}  # fmt: skip
+    done = [0]
+    wall0 = time.perf_counter()
+
+    def run() -> None:
+        # chunks of 250 steps; stop early once the wall time passes the limit (many flagged
+        # points make every step a batched RVE solve)
+        while done[0] < rno_steps:
+            n = min(250, rno_steps - done[0])
+            fe2.run(n)
+            done[0] += n
+            if done[0] < rno_steps:
+                torch.cuda.synchronize()
+                if time.perf_counter() - wall0 > time_limit_s:
+                    break
+
+    rno_ms = _elapsed_ms(run)
+    out = {"points": bar.points, "dt": dt, "rno_steps": done[0], "rno_steps_requested": rno_steps, "rno_ms": rno_ms,
+           "rno_steps_per_s": done[0] / (rno_ms / 1e3), "flagged_points": int(gate.slots_used),
+           "fallback_steps": int(gate.fallback_steps), "simulated_time_s": (rno_warmup + done[0]) * dt}  # fmt: skip
     del fe2, gate
     torch.cuda.empty_cache()
     if direct_steps > 0:

@@ -97,12 +97,14 @@ def impact_paths(
     duration: float = 50.0e-6,
     dt: float | None = None,
     precision: int = 32,
+    point_stride: int = 1,
 ) -> RNODataset:
-    """Macro strain and homogenised stress histories at every macro point of direct FE^2
+    """Macro strain and homogenised stress histories at the macro points of direct FE^2
     bar runs, one run per half-sine pressure amplitude -- the reference's impact_path data
     source (macro paths extracted from direct explicit FE^2,
     src/concrete_impact/experiments/rve_response_generation.py:898-940 and
-    rve_path_generation.py:44-47).  Every macro point gives one path of ``steps`` steps."""
+    rve_path_generation.py:44-47).  Every ``point_stride``-th macro point gives one path of
+    ``steps`` steps (neighbouring points of one run carry nearly the same history)."""
     from .fe2 import DirectRVEPoints, ExplicitFE2, build_macro_bar, half_sine_pressure, stable_time_step
 
     bar = build_macro_bar(divisions, lengths, density)
@@ -112,12 +114,13 @@ def impact_paths(
     for amp in amplitudes:
         fe2 = ExplicitFE2(bar, DirectRVEPoints(model, bar.points, update_settings, precision=precision), dt,
                           lambda t, a=float(amp): half_sine_pressure(t, a, duration))  # fmt: skip
-        e = torch.zeros((bar.points, steps + 1, 6), dtype=torch.float64, device=bar.fixed.device)
+        keep = torch.arange(0, bar.points, point_stride, device=bar.fixed.device)
+        e = torch.zeros((keep.numel(), steps + 1, 6), dtype=torch.float64, device=bar.fixed.device)
         s = torch.zeros_like(e)
         for t in range(1, steps + 1):
             fe2.step()
-            e[:, t] = fe2.strain
-            s[:, t] = fe2.last_stress
+            e[:, t] = fe2.strain[keep]
+            s[:, t] = fe2.last_stress[keep]
         strains.append(e)
         stresses.append(s)
         del fe2
