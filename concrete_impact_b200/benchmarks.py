@@ -280,15 +280,38 @@ def train_fe2_surrogate(recipe: FE2Recipe, log=None):
     return rno, input_envelope(scales, data), info
 
 
-def _record_run(fe2, steps: int) -> tuple[torch.Tensor, torch.Tensor]:
-    """Run ``steps`` steps; (stress (steps, P, 6), displacement (steps, 3N)) at every step."""
+def save_surrogate(path: str, rno, envelope) -> None:
+    """Weights, scales, latent time scale and gate envelope of a trained surrogate."""
+    state = rno.state_dict()
+    state["tau_ref"] = torch.tensor(rno.config.tau_ref, dtype=torch.float64)
+    state["envelope"] = torch.tensor(np.broadcast_arrays(np.asarray(envelope[0], dtype=np.float64).reshape(-1),
+                                                         np.asarray(envelope[1], dtype=np.float64).reshape(-1)))
+    torch.save(state, path)
+
+
+def load_surrogate(path: str):
+    """(rno, envelope) from ``save_surrogate``."""
+    from .rno import RNOConfig, RNOSurrogate
+
+    state = torch.load(path, map_location="cpu")
+    rno = RNOSurrogate(RNOConfig(tau_ref=float(state["tau_ref"])))
+    rno.load_state_dict(state)
+    env = state["envelope"]
+    return rno, (env[0].tolist(), env[1].tolist())
+
+
+def _record_run(fe2, steps: int) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+    """Run ``steps`` steps; (stress (steps, P, 6), displacement (steps, 3N), macro strain
+    (steps, P, 6)) at every step."""
     stress = torch.empty((steps, fe2.bar.points, 6), dtype=torch.float64, device=fe2.u.device)
+    strain = torch.empty_like(stress)
     disp = torch.empty((steps, fe2.u.numel()), dtype=torch.float64, device=fe2.u.device)
     for t in range(steps):
         fe2.step()
         stress[t] = fe2.last_stress
+        strain[t] = fe2.strain
         disp[t] = fe2.u
-    return stress, disp
+    return stress, disp, strain
 
 
 def fe2_accuracy(rno, envelope, steps: int = 400, divisions=(64, 2, 2), precision_direct: int = 64,
@@ -297,6 +320,7 @@ def fe2_accuracy(rno, envelope, steps: int = 400, divisions=(64, 2, 2), precisio
     the same bar (0.01 m elements, half-sine 50 MPa, 50 us): relative Frobenius errors of
     the macro stress and displacement histories."""
     from .fe2 import DirectRVEPoints, ExplicitFE2, RNOPoints, build_macro_bar, stable_time_step
+    from .rno import RNODataset
     from .rno_data import relative_stress_error
 
     model_ref = concrete_rve(8, 0, precision_direct)
@@ -304,13 +328,19 @@ def fe2_accuracy(rno, envelope, steps: int = 400, divisions=(64, 2, 2), precisio
     bar = build_macro_bar(divisions, lengths, 2400.0)
     dt = stable_time_step(bar, model_ref.material.maximum_wave_speed, 0.5)
     direct = ExplicitFE2(bar, DirectRVEPoints(model_ref, bar.points, UPDATE_SETTINGS, precision=precision_direct), dt)
-    s_ref, u_ref = _record_run(direct, steps)
+    s_ref, u_ref, e_ref = _record_run(direct, steps)
     del direct
+    # open loop: the surrogate alone along the direct run's macro strain histories
+    zeros = torch.zeros((bar.points, 1, 6), dtype=torch.float64, device=e_ref.device)
+    paths = RNODataset(torch.cat([zeros, e_ref.transpose(0, 1)], dim=1), torch.cat([zeros, s_ref.transpose(0, 1)], dim=1),
+                       torch.full((bar.points, steps), dt, dtype=torch.float64, device=e_ref.device))  # fmt: skip
+    open_loop = relative_stress_error(rno.rollout(paths), paths.stress[:, 1:])
     gate = RNOPoints(rno, bar.points, envelope, concrete_rve(8, 0, 32), UPDATE_SETTINGS,
                      fallback_capacity=fallback_capacity or bar.points)  # fmt: skip
     surrogate = ExplicitFE2(bar, gate, dt)
-    s_rno, u_rno = _record_run(surrogate, steps)
+    s_rno, u_rno, _ = _record_run(surrogate, steps)
     return {"steps": steps, "divisions": list(divisions), "dt": dt, "points": bar.points,
+            "homogenised_stress_error_open_loop": open_loop,
             "stress_error": relative_stress_error(s_rno, s_ref), "displacement_error": relative_stress_error(u_rno, u_ref),
             "flagged_points": int(gate.slots_used), "fallback_steps": int(gate.fallback_steps),
             "stress_rms_pa": float(s_ref.pow(2).mean().sqrt().item())}  # fmt: skip

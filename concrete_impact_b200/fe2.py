@@ -154,9 +154,10 @@ class DirectRVEPoints:
 class RNOPoints:
     """The surrogate at every macro point, with an input-envelope gate and a direct fallback.
 
-    ``envelope`` = (max |normalised strain|, max |normalised rate|) seen in training; a point
-    whose input exceeds ``envelope_factor`` times it is flagged and solved by a fallback RVE
-    from then on (at most ``fallback_capacity`` points).
+    ``envelope`` = (max |normalised strain|, max |normalised rate|) seen in training, each a
+    scalar or a 6-vector of per-component maxima; a point any of whose input components
+    exceeds ``envelope_factor`` times its limit is flagged and solved by a fallback RVE from
+    then on (at most ``fallback_capacity`` points).
     """
 
     def __init__(self, rno: RNOSurrogate, n_points: int, envelope: tuple[float, float],
@@ -169,6 +170,7 @@ class RNOPoints:
         self.z_next = self.z
         self.envelope = envelope
         self.factor = envelope_factor
+        self._lim = None
         self.model = model
         self.settings = update_settings
         self.buffers = None
@@ -190,8 +192,8 @@ class RNOPoints:
         stress = out.double()
         if self.pool is None:
             return stress
-        over = ((strain.abs() / s.strain).amax(dim=1) > self.factor * self.envelope[0]) | (
-            (rate.abs() / s.rate).amax(dim=1) > self.factor * self.envelope[1])  # fmt: skip
+        lim_e, lim_r = self._limits(strain.device)
+        over = ((strain.abs() / s.strain) > lim_e).any(dim=1) | ((rate.abs() / s.rate) > lim_r).any(dim=1)
         new = over & ~self.flagged
         if bool(new.any()):
             self._admit(torch.nonzero(new).flatten(), strain)
@@ -212,6 +214,14 @@ class RNOPoints:
             stress[pts] = self.pool.sums[used, RS_SIGMA : RS_SIGMA + 6] / vol
             self.fallback_steps += 1
         return stress
+
+    def _limits(self, device) -> tuple[torch.Tensor, torch.Tensor]:
+        """Gate limits per component (scalars broadcast to all six)."""
+        if self._lim is None:
+            e = torch.as_tensor(self.envelope[0], dtype=torch.float64, device=device).reshape(-1)
+            r = torch.as_tensor(self.envelope[1], dtype=torch.float64, device=device).reshape(-1)
+            self._lim = (self.factor * e, self.factor * r)
+        return self._lim
 
     def _admit(self, points: torch.Tensor, strain: torch.Tensor) -> None:
         """Give newly flagged points a fallback RVE from the zero state; the first solve of

@@ -354,9 +354,13 @@ class RNOSurrogate:
         return float(w["loss_part"].sum().item()) / float(w["B"] * w["T"] * 6)
 
     # -- training -----------------------------------------------------------------------
-    def fit(self, data: RNODataset, epochs: int, graph: bool = True, log=None, lr_schedule=None) -> list[float]:
+    def fit(self, data: RNODataset, epochs: int, graph: bool = True, log=None, lr_schedule=None,
+            input_noise: float = 0.0) -> list[float]:  # fmt: skip
         """Train on ``data`` (device-resident); returns the mean loss per epoch.
-        ``lr_schedule(epoch)``, when given, sets the step size of each epoch."""
+        ``lr_schedule(epoch)``, when given, sets the step size of each epoch.  ``input_noise``
+        adds N(0, input_noise^2) to the normalised strain and rate inputs of every window
+        (targets unchanged): the network is taught to be insensitive to input perturbations
+        of that size, which keeps its response smooth where a macro solver drives it."""
         c = self.config
         P, T = data.paths, data.steps
         rates = data.rates()
@@ -370,6 +374,7 @@ class RNOSurrogate:
         if T % W != 0:
             raise ValueError("the path length must be a multiple of the truncation window")
         gen = torch.Generator(device="cpu").manual_seed(c.seed)
+        noise_gen = torch.Generator(device=self.device).manual_seed(c.seed + 1)
         history = []
         for epoch in range(epochs):
             if lr_schedule is not None:
@@ -382,8 +387,11 @@ class RNOSurrogate:
                 z0 = torch.zeros((B, 6), dtype=torch.float32, device=self.device)
                 for t0 in range(0, T, W):
                     sl = slice(t0, t0 + W)
-                    self.load_window(strain_n[idx, sl].transpose(0, 1), rate_n[idx, sl].transpose(0, 1),
-                                     stress_n[idx, sl].transpose(0, 1), coef[idx, sl].transpose(0, 1), z0)  # fmt: skip
+                    xs, xr = strain_n[idx, sl].transpose(0, 1), rate_n[idx, sl].transpose(0, 1)
+                    if input_noise > 0.0:
+                        xs = xs + input_noise * torch.randn(xs.shape, device=xs.device, generator=noise_gen)
+                        xr = xr + input_noise * torch.randn(xr.shape, device=xr.device, generator=noise_gen)
+                    self.load_window(xs, xr, stress_n[idx, sl].transpose(0, 1), coef[idx, sl].transpose(0, 1), z0)
                     if graph:
                         self._replay(W, B)
                     else:

@@ -142,9 +142,14 @@ def split_dataset(data: RNODataset, validation: int) -> tuple[RNODataset, RNODat
             RNODataset(data.strain[k:], data.stress[k:], data.dt[k:]))  # fmt: skip
 
 
-def input_envelope(scales: RNOScales, data: RNODataset) -> tuple[float, float]:
+def input_envelope(scales: RNOScales, data: RNODataset, per_component: bool = False):
     """(max |normalised strain|, max |normalised rate|) over the training paths: the region
-    in which the surrogate's answers are trusted by the macro error gate."""
+    in which the surrogate's answers are trusted by the macro error gate.  With
+    ``per_component`` each entry is a list of the six component maxima."""
+    if per_component:
+        strain = (data.strain.abs().amax(dim=(0, 1)) / scales.strain).tolist()
+        rate = (data.rates().abs().amax(dim=(0, 1)) / scales.rate).tolist()
+        return strain, rate
     strain = float((data.strain.abs().amax() / scales.strain).item())
     rate = float((data.rates().abs().amax() / scales.rate).item())
     return strain, rate
