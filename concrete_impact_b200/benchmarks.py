@@ -230,19 +230,22 @@ def rno_training_workload(paths: int = 2000, steps: int = 200, epochs: int = 300
 
 @dataclass(frozen=True)
 class FE2Recipe:
-    """How the deployed surrogate is trained: random RVE paths plus impact paths taken from
-    direct FE^2 runs of a calibration bar at other pulse amplitudes (the reference's
+    """How the deployed surrogate is trained: random 6-component RVE paths (general states;
+    they also keep the surrogate stable when a macro solver drives it) plus impact paths taken
+    from direct FE^2 runs of a calibration bar at other pulse amplitudes (the reference's
     impact_path data source)."""
 
-    random_paths: int = 0
+    random_paths: int = 2000
+    random_amplitude: tuple[float, float] = (2.0e-4, 5.0e-3)
     path_steps: int = 400
     impact_amplitudes: tuple[float, ...] = (20.0e6, 30.0e6, 40.0e6, 60.0e6, 70.0e6, 80.0e6)
     calibration_divisions: tuple[int, int, int] = (64, 2, 2)
-    point_stride: int = 4
-    epochs: int = 1000
-    tau_ref: float = 1.0e-5
+    point_stride: int = 2
+    epochs: int = 1500
+    tau_ref: float = 1.0e-4
     learning_rate: float = 1.0e-3
     final_lr_fraction: float = 0.02
+    input_noise: float = 0.0
 
 
 def train_fe2_surrogate(recipe: FE2Recipe, log=None):
@@ -257,8 +260,8 @@ def train_fe2_surrogate(recipe: FE2Recipe, log=None):
     t0 = time.perf_counter()
     sets = []
     if recipe.random_paths:
-        sets.append(generate_rve_paths(model32, PathSetSpec(recipe.random_paths, recipe.path_steps, seed=20000),
-                                       UPDATE_SETTINGS, precision=32))  # fmt: skip
+        spec = PathSetSpec(recipe.random_paths, recipe.path_steps, seed=20000, amplitude=tuple(recipe.random_amplitude))
+        sets.append(generate_rve_paths(model32, spec, UPDATE_SETTINGS, precision=32))
     if recipe.impact_amplitudes:
         lengths = tuple(0.01 * d for d in recipe.calibration_divisions)
         sets.append(impact_paths(model32, recipe.impact_amplitudes, recipe.path_steps, UPDATE_SETTINGS,
@@ -273,19 +276,19 @@ def train_fe2_surrogate(recipe: FE2Recipe, log=None):
     lr0, frac, E = recipe.learning_rate, recipe.final_lr_fraction, recipe.epochs
     schedule = lambda e: lr0 * (frac + (1.0 - frac) * 0.5 * (1.0 + math.cos(math.pi * e / max(E, 1))))  # noqa: E731
     t0 = time.perf_counter()
-    history = rno.fit(data, E, lr_schedule=schedule, log=log)
+    history = rno.fit(data, E, lr_schedule=schedule, log=log, input_noise=recipe.input_noise)
     torch.cuda.synchronize()
     info["training_s"] = time.perf_counter() - t0
     info["loss_first_last"] = [history[0], history[-1]] if history else None
-    return rno, input_envelope(scales, data), info
+    return rno, input_envelope(scales, data, per_component=True), info
 
 
 def save_surrogate(path: str, rno, envelope) -> None:
     """Weights, scales, latent time scale and gate envelope of a trained surrogate."""
     state = rno.state_dict()
     state["tau_ref"] = torch.tensor(rno.config.tau_ref, dtype=torch.float64)
-    state["envelope"] = torch.tensor(np.broadcast_arrays(np.asarray(envelope[0], dtype=np.float64).reshape(-1),
-                                                         np.asarray(envelope[1], dtype=np.float64).reshape(-1)))
+    e, r = (np.asarray(v, dtype=np.float64).reshape(-1) for v in envelope)
+    state["envelope"] = torch.as_tensor(np.stack(np.broadcast_arrays(e, r)))
     torch.save(state, path)
 
 
