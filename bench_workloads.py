@@ -281,11 +281,19 @@ def run_fe2(args: argparse.Namespace) -> None:
     FE^2 (FP64 RVEs) on a 64x2x2 bar, then time surrogate FE^2 on the 64x16x16 bar for
     ``--steps`` macro steps and all-direct FE^2 (FP32 RVEs) on the same bar for a short
     window from rest.  CIB_FE2_RECIPE (JSON of FE2Recipe fields), CIB_FE2_ACCURACY_STEPS and
-    CIB_FE2_DIRECT_STEPS override the defaults."""
+    CIB_FE2_DIRECT_STEPS override the defaults; CIB_FE2_SAVE / CIB_FE2_LOAD store or reuse
+    the trained surrogate."""
     import torch
 
     from bench import ClockSampler
-    from concrete_impact_b200.benchmarks import FE2Recipe, fe2_accuracy, fe2_speed, train_fe2_surrogate
+    from concrete_impact_b200.benchmarks import (
+        FE2Recipe,
+        fe2_accuracy,
+        fe2_speed,
+        load_surrogate,
+        save_surrogate,
+        train_fe2_surrogate,
+    )
 
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -293,7 +301,13 @@ def run_fe2(args: argparse.Namespace) -> None:
     fields = json.loads(os.environ.get("CIB_FE2_RECIPE", "{}"))
     recipe = FE2Recipe(**{k: tuple(v) if isinstance(v, list) else v for k, v in fields.items()})
     t0 = time.perf_counter()
-    rno, envelope, info = train_fe2_surrogate(recipe)
+    if os.environ.get("CIB_FE2_LOAD"):
+        rno, envelope = load_surrogate(os.environ["CIB_FE2_LOAD"])
+        info = {"loaded": os.environ["CIB_FE2_LOAD"]}
+    else:
+        rno, envelope, info = train_fe2_surrogate(recipe)
+        if os.environ.get("CIB_FE2_SAVE"):
+            save_surrogate(os.environ["CIB_FE2_SAVE"], rno, envelope)
     _progress("trained", time.perf_counter() - t0, info)
     acc = fe2_accuracy(rno, envelope, steps=int(os.environ.get("CIB_FE2_ACCURACY_STEPS", "400")))
     _progress("accuracy", time.perf_counter() - t0, acc)
