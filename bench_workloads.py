@@ -192,10 +192,11 @@ def run_rve_batch(args: argparse.Namespace) -> None:
                   "accepted_rve_steps_per_s": rve_steps_s, "elements": out["elements"],
                   "gauss_points": out["gauss_points"], "newton_max": out["newton_max"], "pcg_max": out["pcg_max"],
                   "pcg_total": out["pcg_total"], "plastic_fraction": out["plastic_fraction"],
+                  "pcg_cluster": out["pcg_cluster"], "pcg_cluster_tuning_ms": (out["tuning"] or {}).get("ms"),
                   "kernel_ms": out["kernel_ms"], "kernel_launches": out["kernel_launches"],
                   "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                "frac": None if achieved is None else achieved / peak, "traffic": None,
-                               "peak_kind": kind, "kernel": "rve_pcg_kernel<float>",
+                               "peak_kind": kind, "kernel": "rve_pcg_cluster_kernel<float> (rve_pcg_kernel at cluster 1)",
                                "algorithmic_bytes": pcg_bytes,
                                "note": "algorithmic bytes of all PCG iterations over the PCG launches' event time; "
                                        "small RVEs stay in L2"},

@@ -195,6 +195,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_rve_residual": (_I, [_P] * 9),
     "cib_rve_gather": (_I, [_P] * 12),
     "cib_rve_pcg": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32] + [_P] * 5),
+    "cib_rve_pcg_cluster": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32, ctypes.c_int32] + [_P] * 5),
     "cib_rve_pcg_noalloc": (_I, [_P, ctypes.c_int32, _P, _P, _P, _I64, _P, _P, _P, _D, ctypes.c_int32] + [_P] * 5),
     "cib_rve_tangent_rhs": (_I, [_P] * 6),
     "cib_rve_tangent_finish": (_I, [_P] * 7),

@@ -39,6 +39,7 @@ from .rve import (
     initialize_rve_state,
     solve_batch_step,
     solve_rve_microequilibrium,
+    tune_pcg_cluster,
 )
 from .rve_builders import (
     build_two_phase_sphere_rve,
@@ -129,11 +130,13 @@ def rve_batch_setup(n_rve: int = 256, steps: int = 200, edges=EDGES, base_seed: 
     return RVEBatchSetup(models, np.asarray(times), np.asarray(strains))
 
 
-def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision: int = 32) -> dict:
+def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision: int = 32, tune: bool = True) -> dict:
     """Advance every RVE of the batch ``warmup`` path steps untimed, then ``timed`` steps
     timed; one step = one batched Newton solve (+ homogenisation and commit) per time index.
     Each step copies its macro strains and time steps from pinned host memory and reads the
-    homogenised stresses back (the caller's view of the batched API)."""
+    homogenised stresses back (the caller's view of the batched API).  With ``tune`` the PCG
+    cluster size is measured (``tune_pcg_cluster``) on the first timed step's system before
+    the timed region."""
     batch = RVEBatch(setup.models, precision=precision)
     dev = batch.device
     strain_h = torch.as_tensor(setup.strains).pin_memory()
@@ -162,6 +165,11 @@ def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision:
 
     for t in range(1, warmup + 1):
         step(t, False)
+    tuning = None
+    if tune:
+        batch.macro.copy_(strain_h[:, warmup + 1])
+        batch.dt.copy_(dt_h[:, warmup])
+        tuning = tune_pcg_cluster(batch, UPDATE_SETTINGS)
     ms = _elapsed_ms(lambda: [step(t, True) for t in range(warmup + 1, warmup + timed + 1)])
     kernel_ms = {k: float(sum(a.elapsed_time(b) for a, b in v)) for k, v in timers.items()}
     launches = {k: len(v) for k, v in timers.items()}
@@ -169,7 +177,8 @@ def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision:
     return {"ms": ms, "rve_steps": batch.nrve * timed, "gauss_points": int(gp.sum()), "elements": int(batch.nelem),
             "stress_last": stress_h.numpy().copy(), "kernel_ms": kernel_ms, "kernel_launches": launches,
             "plastic_fraction": plastic, "h2d_bytes_per_step": int(batch.nrve * 7 * 8),
-            "d2h_bytes_per_step": int(batch.nrve * 6 * 8), **counts}  # fmt: skip
+            "d2h_bytes_per_step": int(batch.nrve * 6 * 8), "pcg_cluster": int(batch.cluster), "tuning": tuning,
+            **counts}  # fmt: skip
 
 
 # ---------------------------------------------------------------------------------------

@@ -25,9 +25,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cooperative_groups.h>
+
 #include "cib_common.cuh"
 #include "j2vp_point.cuh"
 #include "rve.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace cib {
 
@@ -637,6 +641,245 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_pcg_kernel(const RvePcgArgs<T
 }
 
 // ---------------------------------------------------------------------------------------
+// Cluster variant of the PCG: C CTAs of one thread-block cluster share one system.  Rank q
+// owns the node layers [k0, k1) = [q nz / C, (q + 1) nz / C) of its RVE: it streams its
+// element layers like apply_tangent, keeps the bottom contributions of its first node layer
+// (acc_first) and exports the top contributions of its last element layer, which belong to
+// the next rank's first node layer (the last rank's wrap to node layer 0 is the periodic
+// closure); after a cluster barrier every rank adds its predecessor's export through
+// distributed shared memory.  Dot products are CTA sums combined over the ranks in rank
+// order (every rank forms the same totals, so all ranks take the same branches).  Four
+// cluster barriers per iteration: export, p.Ap, r.r / r.z, and p visibility.  With C = 1
+// the arithmetic and its order are those of rve_pcg_kernel.
+template <typename T>
+__device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, const double* __restrict__ p,
+                                     double* __restrict__ Ap, double* smem, int k0, int k1,
+                                     cg::cluster_group& cl, unsigned prev_rank) {
+  const int nxy = d.nx * d.ny;
+  double* ye = smem;                  // nxy * 24
+  double* acc_cur = ye + 24 * nxy;    // nxy * 3
+  double* acc_next = acc_cur + 3 * nxy;
+  double* acc_first = acc_next + 3 * nxy;
+  double* exported = acc_first + 3 * nxy;
+  const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
+  double pap = 0.0;
+  const int items = 8 * nxy;
+  const int rounds = (items + blockDim.x - 1) / blockDim.x;
+  for (int k = k0; k < k1; ++k) {
+    for (int it = 0; it < rounds; ++it) {
+      const int gl = it * blockDim.x + threadIdx.x;
+      const bool live = gl < items;
+      const int el = live ? (gl >> 3) : 0;
+      const int q = gl & 7;
+      const int i = el % d.nx, j = el / d.nx;
+      const int64_t e = d.eoff + el + (int64_t)nxy * k;
+      T mine[3] = {0, 0, 0};
+      if (live) {
+        const int64_t node = element_node(d, i, j, k, q);
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) mine[dd] = (T)__ldcg(p + 3 * node + dd);  // other ranks wrote p
+      }
+      T u[8][3];
+      allgather8(mine, u);
+      Grad8<T> Gr;
+      physical_grads(q, d, Gr);
+      T eps[6], sig[6];
+      strain_from(Gr, u, eps);
+      const int64_t g = 8 * e + q;
+      const int ph = live ? (int)a.phase[e] : 0;
+      TangentParams<T> tp;
+      tp.elastic = 1;
+      tp.f = (T)0;
+      tp.c = (T)0;
+      if (live && a.tflag[g]) {
+        tp.elastic = 0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) tp.n[c] = a.tparam[c * a.ngp + g];
+        tp.f = a.tparam[6 * a.ngp + g];
+        tp.c = a.tparam[7 * a.ngp + g];
+      }
+      tangent_apply(a.mats.m[ph], tp, eps, sig);
+      T f[8][3];
+      bt_stress(Gr, sig, live ? jw : (T)0, f);
+      T out[3];
+      reduce_scatter8(f, q, out);
+      if (live)
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) ye[(8 * el + q) * 3 + dd] = (double)out[dd];
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
+      const int i = n % d.nx, j = n / d.nx;
+      double bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
+      for (int s = 0; s < 4; ++s) {
+        const int di = s & 1, dj = s >> 1;
+        const int el = (i - di + d.nx) % d.nx + d.nx * ((j - dj + d.ny) % d.ny);
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+          bot[dd] += ye[(8 * el + s) * 3 + dd];
+          top[dd] += ye[(8 * el + s + 4) * 3 + dd];
+        }
+      }
+      if (k == k0) {
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) acc_first[3 * n + dd] = bot[dd];
+      } else {
+        const int64_t node = d.eoff + n + (int64_t)nxy * k;
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+          const double v = acc_cur[3 * n + dd] + bot[dd];
+          Ap[3 * node + dd] = v;
+          pap += p[3 * node + dd] * v;
+        }
+      }
+      if (k == k1 - 1) {
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) exported[3 * n + dd] = top[dd];
+      } else {
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) acc_next[3 * n + dd] = top[dd];
+      }
+    }
+    __syncthreads();
+    double* t = acc_cur;
+    acc_cur = acc_next;
+    acc_next = t;
+  }
+  cl.sync();  // every rank's export is complete
+  const double* prev = cl.map_shared_rank(exported, prev_rank);
+  for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
+    const int64_t node = d.eoff + n + (int64_t)nxy * k0;
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      const double v = (k0 == 0 && n == 0) ? 0.0 : acc_first[3 * n + dd] + prev[3 * n + dd];
+      Ap[3 * node + dd] = v;
+      pap += p[3 * node + dd] * v;
+    }
+  }
+  return pap;
+}
+
+// Sum of NV doubles over the CTAs of the cluster, the same on every thread of every rank.
+// `slots` (NV doubles of this CTA's shared memory) must not be rewritten before the next
+// cluster barrier that follows every rank's read.
+template <int NV>
+__device__ __forceinline__ void cluster_sum(double (&v)[NV], double* scratch, double* slots, cg::cluster_group& cl) {
+  block_sum<NV>(v, scratch);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) slots[k] = v[k];
+  cl.sync();
+  double t[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) t[k] = 0.0;
+  const unsigned nr = cl.num_blocks();
+  for (unsigned q = 0; q < nr; ++q) {
+    const double* rem = cl.map_shared_rank(slots, q);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) t[k] += rem[k];
+  }
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = t[k];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RVE_THREADS) rve_pcg_cluster_kernel(const RvePcgArgs<T> a) {
+  extern __shared__ double smem[];
+  __shared__ double scratch[64];
+  __shared__ double slot_init[2], slot_pap[1], slot_rr[2], slot_xn[1];
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned C = cl.num_blocks();
+  const unsigned rank = cl.block_rank();
+  const int s = blockIdx.x / C;
+  const int r = a.sys_rve[s];
+  if (a.active && !a.active[r]) return;  // the whole cluster leaves together
+  const RveDesc d = a.desc[r];
+  if (d.nz < (int)C) {  // every rank must own a layer
+    if (rank == 0 && threadIdx.x == 0) {
+      a.status[s] = 3;
+      a.iterations[s] = 0;
+      a.rel_residual[s] = 0.0;
+      a.xnorm[s] = 0.0;
+    }
+    return;
+  }
+  const int nxy = d.nx * d.ny;
+  const int k0 = (int)((rank * (unsigned)d.nz) / C), k1 = (int)(((rank + 1) * (unsigned)d.nz) / C);
+  const unsigned prev_rank = (rank + C - 1) % C;
+  const int64_t off = a.sys_off[s];
+  const int64_t shift = 3 * d.eoff;
+  const int64_t lo = 3 * (int64_t)nxy * k0, hi = 3 * (int64_t)nxy * k1;  // this rank's vector entries
+  const double* b = a.b + off;
+  double* x = a.x + off;
+  double* rr = a.r + off;
+  double* p = a.p + off;
+  double* Ap = a.Ap + off;
+  const double* dinv = a.dinv + 3 * d.eoff;
+  double v[2] = {0.0, 0.0};  // r.z, b.b
+  for (int64_t n = lo + threadIdx.x; n < hi; n += blockDim.x) {
+    const double bi = b[n];
+    x[n] = 0.0;
+    rr[n] = bi;
+    const double z = dinv[n] * bi;
+    p[n] = z;
+    v[0] += bi * z;
+    v[1] += bi * bi;
+  }
+  cluster_sum<2>(v, scratch, slot_init, cl);  // its barrier also publishes p
+  double rz = v[0];
+  const double bnorm = sqrt(v[1]);
+  const double tol = a.rtol * bnorm;
+  int status = 1, iters = 0;
+  double rnorm = bnorm;
+  if (bnorm == 0.0 || !(bnorm == bnorm)) {
+    status = (bnorm == 0.0) ? 0 : 2;
+  } else {
+    for (iters = 0; iters < a.maxit;) {
+      double pap[1] = {apply_tangent_slab<T>(a, d, p - shift, Ap - shift, smem, k0, k1, cl, prev_rank)};
+      cluster_sum<1>(pap, scratch, slot_pap, cl);
+      if (!(pap[0] > 0.0) || !isfinite(pap[0])) {
+        status = 2;
+        break;
+      }
+      const double alpha = rz / pap[0];
+      double w2[2] = {0.0, 0.0};  // r.r, r.z
+      for (int64_t n = lo + threadIdx.x; n < hi; n += blockDim.x) {
+        x[n] += alpha * p[n];
+        const double rn = rr[n] - alpha * Ap[n];
+        rr[n] = rn;
+        w2[0] += rn * rn;
+        w2[1] += rn * dinv[n] * rn;
+      }
+      cluster_sum<2>(w2, scratch, slot_rr, cl);
+      ++iters;
+      rnorm = sqrt(w2[0]);
+      if (!isfinite(rnorm)) {
+        status = 2;
+        break;
+      }
+      if (rnorm <= tol) {
+        status = 0;
+        break;
+      }
+      const double beta = w2[1] / rz;
+      rz = w2[1];
+      for (int64_t n = lo + threadIdx.x; n < hi; n += blockDim.x) p[n] = dinv[n] * rr[n] + beta * p[n];
+      cl.sync();  // p of every rank visible before the next apply
+    }
+  }
+  double xn[1] = {0.0};
+  for (int64_t n = lo + threadIdx.x; n < hi; n += blockDim.x) xn[0] += x[n] * x[n];
+  cluster_sum<1>(xn, scratch, slot_xn, cl);
+  if (rank == 0 && threadIdx.x == 0) {
+    a.status[s] = status;
+    a.iterations[s] = iters;
+    a.rel_residual[s] = bnorm > 0.0 ? rnorm / bnorm : 0.0;
+    a.xnorm[s] = sqrt(xn[0]);
+  }
+  cl.sync();  // no rank leaves while another may still read its shared memory
+}
+
+// ---------------------------------------------------------------------------------------
 // Right-hand sides of the effective-tangent solves and K_ee.  For macro strain unit j,
 // element forces f_e^(j) = sum_q w B_q^T C_q e_j; gathered periodically they give column j
 // of K_we = T^T K A; K_ee = A^T K A = sum_q w C_q (since B_q A e_j = e_j on a box).
@@ -1052,6 +1295,36 @@ int launch_rve_pcg(const RvePcgArgs<T>& a, int nsys, int max_nxy, cudaStream_t s
 }
 
 template <typename T>
+int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cluster, cudaStream_t st) {
+  if (cluster == 1) return launch_rve_pcg<T>(a, nsys, max_nxy, st);
+  if (cluster != 2 && cluster != 4 && cluster != 8) return CIB_EINVAL;
+  const size_t smem = (size_t)max_nxy * (24 + 12) * sizeof(double);
+  if (smem > 200 * 1024) return CIB_ERANGE;
+  static bool configured[2] = {false, false};
+  const int slot = sizeof(T) == 8 ? 1 : 0;
+  if (!configured[slot]) {
+    if (cudaFuncSetAttribute(rve_pcg_cluster_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+        cudaSuccess)
+      return check_launch();
+    configured[slot] = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)nsys * (unsigned)cluster, 1, 1);
+  cfg.blockDim = dim3(RVE_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, rve_pcg_cluster_kernel<T>, a);
+  return check_launch();
+}
+
+template <typename T>
 int launch_rve_tangent_rhs(const RveTangentArgs<T>& a, int nrve, cudaStream_t st) {
   rve_tangent_rhs_kernel<T><<<nrve, RVE_THREADS, 0, st>>>(a);
   return check_launch();
@@ -1072,6 +1345,8 @@ template int launch_rve_residual<float>(const RveResidualArgs<float>&, int, cuda
 template int launch_rve_residual<double>(const RveResidualArgs<double>&, int, cudaStream_t);
 template int launch_rve_pcg<float>(const RvePcgArgs<float>&, int, int, cudaStream_t);
 template int launch_rve_pcg<double>(const RvePcgArgs<double>&, int, int, cudaStream_t);
+template int launch_rve_pcg_cluster<float>(const RvePcgArgs<float>&, int, int, int, cudaStream_t);
+template int launch_rve_pcg_cluster<double>(const RvePcgArgs<double>&, int, int, int, cudaStream_t);
 template int launch_rve_tangent_rhs<float>(const RveTangentArgs<float>&, int, cudaStream_t);
 template int launch_rve_tangent_rhs<double>(const RveTangentArgs<double>&, int, cudaStream_t);
 template int launch_rve_response<float>(const RveResponseArgs<float>&, int, cudaStream_t);

@@ -175,6 +175,8 @@ int launch_rve_gather(const RveGatherArgs& a, int nrve, cudaStream_t st);
 template <typename T>
 int launch_rve_pcg(const RvePcgArgs<T>& a, int nsys, int max_nxy, cudaStream_t st);
 template <typename T>
+int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cluster, cudaStream_t st);
+template <typename T>
 int launch_rve_tangent_rhs(const RveTangentArgs<T>& a, int nrve, cudaStream_t st);
 int launch_rve_tangent_finish(const RveTangentFinishArgs& a, int nrve, cudaStream_t st);
 template <typename T>

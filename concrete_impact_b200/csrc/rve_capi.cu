@@ -68,7 +68,8 @@ int residual_t(const cib_rve_batch& b, const double* dt, const double* macro, co
 template <typename T>
 int pcg_t(const cib_rve_batch& b, int32_t nsys, const int32_t* sys_rve, const int64_t* sys_off, const int32_t* active,
           const double* rhs, const double* dinv, double* x, double* r, double* p, double* Ap, double rtol,
-          int32_t maxit, int32_t* status, int32_t* iterations, double* rel, double* xnorm, cudaStream_t st) {
+          int32_t maxit, int32_t* status, int32_t* iterations, double* rel, double* xnorm, cudaStream_t st,
+          int32_t cluster = 1) {
   RvePcgArgs<T> a;
   a.desc = reinterpret_cast<const RveDesc*>(b.desc);
   a.phase = b.phase;
@@ -91,7 +92,7 @@ int pcg_t(const cib_rve_batch& b, int32_t nsys, const int32_t* sys_rve, const in
   a.iterations = iterations;
   a.rel_residual = rel;
   a.xnorm = xnorm;
-  return launch_rve_pcg<T>(a, nsys, b.max_nxy, st);
+  return launch_rve_pcg_cluster<T>(a, nsys, b.max_nxy, cluster, st);
 }
 
 template <typename T>
@@ -195,6 +196,24 @@ extern "C" int cib_rve_pcg(const cib_rve_batch* batch, int32_t nsys, const int32
                              iterations, rel_residual, xnorm, st)
              : pcg_t<float>(*batch, nsys, sys_rve, sys_off, active, b, dinv, x, r, p, Ap, rtol, maxit, status,
                             iterations, rel_residual, xnorm, st);
+}
+
+extern "C" int cib_rve_pcg_cluster(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve,
+                                   const int64_t* sys_off, const int32_t* active, const double* b, const double* dinv,
+                                   double* x, double* r, double* p, double* Ap, double rtol, int32_t maxit,
+                                   int32_t cluster, int32_t* status, int32_t* iterations, double* rel_residual,
+                                   double* xnorm, void* stream) {
+  if (!batch_ok(batch) || nsys < 0 || !sys_rve || !sys_off || !b || !dinv || !x || !r || !p || !Ap || !status ||
+      !iterations || !rel_residual || !xnorm || maxit < 0 || !batch->tparam || !batch->tflag || batch->max_nxy <= 0 ||
+      (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8))
+    return CIB_EINVAL;
+  if (nsys == 0) return CIB_OK;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  return batch->precision == 64
+             ? pcg_t<double>(*batch, nsys, sys_rve, sys_off, active, b, dinv, x, r, p, Ap, rtol, maxit, status,
+                             iterations, rel_residual, xnorm, st, cluster)
+             : pcg_t<float>(*batch, nsys, sys_rve, sys_off, active, b, dinv, x, r, p, Ap, rtol, maxit, status,
+                            iterations, rel_residual, xnorm, st, cluster);
 }
 
 extern "C" int cib_rve_tangent_rhs(const cib_rve_batch* batch, const int32_t* active, double* fe6, double* rhs,

@@ -191,10 +191,13 @@ class NonlinearNewtonSettings:
 class LinearSolverOptions:
     """Matrix-free PCG controls of the reduced tangent solves (no reference counterpart:
     the reference solves directly).  ``relative_tolerance`` None picks 1e-11 for float64
-    element kernels and 1e-6 for float32."""
+    element kernels and 1e-6 for float32.  ``cluster`` is the number of CTAs (1, 2, 4, 8;
+    one thread-block cluster) that share each linear system, or "auto" for a choice from
+    the batch's RVE sizes; ``tune_pcg_cluster`` measures the choice instead."""
 
     relative_tolerance: float | None = None
     max_iterations: int = 5000
+    cluster: int | str = 1
 
 
 @dataclass(frozen=True)
@@ -433,6 +436,9 @@ class RVEBatch:
         self.sys_off = torch.as_tensor(3 * self.elem_offsets, device=dev)
         self._tangent_buffers = None
         self.settings = MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10)
+        self.min_nz = int(min(m.divisions[2] for m in models))
+        c = self.linear.cluster
+        self.cluster = auto_pcg_cluster(self) if c == "auto" else self.check_cluster(int(c))
         self._batch_struct = None
 
     # -- C structs ---------------------------------------------------------------------
@@ -476,14 +482,21 @@ class RVEBatch:
         )  # fmt: skip
         _native.check(code, "cib_rve_gather")
 
+    def check_cluster(self, cluster: int) -> int:
+        if cluster not in (1, 2, 4, 8):
+            raise ValueError("the PCG cluster size must be 1, 2, 4 or 8")
+        if cluster > self.min_nz:
+            raise ValueError(f"PCG cluster {cluster} needs every RVE to have at least {cluster} element layers in z")
+        return cluster
+
     def pcg(self, b, rhs: torch.Tensor, x, r, p, Ap, nsys: int, sys_rve, sys_off, status, iters, rel, xnorm) -> None:
-        code = self.lib.cib_rve_pcg(
+        code = self.lib.cib_rve_pcg_cluster(
             ctypes.byref(b), nsys, sys_rve.data_ptr(), sys_off.data_ptr(), self.active.data_ptr(), rhs.data_ptr(),
             self.dinv.data_ptr(), x.data_ptr(), r.data_ptr(), p.data_ptr(), Ap.data_ptr(), float(self.rtol),
-            int(self.linear.max_iterations), status.data_ptr(), iters.data_ptr(), rel.data_ptr(), xnorm.data_ptr(),
-            _native.stream_ptr(),
+            int(self.linear.max_iterations), int(self.cluster), status.data_ptr(), iters.data_ptr(), rel.data_ptr(),
+            xnorm.data_ptr(), _native.stream_ptr(),
         )  # fmt: skip
-        _native.check(code, "cib_rve_pcg")
+        _native.check(code, "cib_rve_pcg_cluster")
 
     def effective_tangent(self, b) -> torch.Tensor:
         """(R, 6, 6) condensed tangent of the last residual pass (solver.py:438-461)."""
@@ -634,6 +647,43 @@ def solve_batch_step(
     else:
         _set_active(batch, final_active)
     return BatchStepResult(iters_out, backtracks, res_out, tol_out, pcg_total)
+
+
+def auto_pcg_cluster(batch: RVEBatch) -> int:
+    """Cluster size from the batch's sizes: doubled while the largest RVE has at least
+    2 x 1,728 elements (a 12^3 block) per CTA, at most 8 and at most the smallest number
+    of z layers."""
+    largest = int(batch.elem_counts.max())
+    c = 1
+    while c < 8 and 2 * c <= batch.min_nz and largest >= 1728 * 2 * c:
+        c *= 2
+    return c
+
+
+def tune_pcg_cluster(batch: RVEBatch, update_settings: MaterialUpdateSettings, candidates=(1, 2, 4, 8)) -> dict:
+    """Time one PCG solve of the batch's current Newton system (a residual pass at the
+    committed fluctuation) for each admissible cluster size and keep the fastest.  The
+    solves write only work vectors; the batch's state is unchanged.  Returns
+    {"cluster": best, "ms": {size: milliseconds}}."""
+    b = batch.batch_struct(update_settings)
+    saved = batch.cluster
+    batch.w.copy_(batch.w_n)
+    batch.residual(b, batch.w, None, None)
+    timings = {}
+    for c in candidates:
+        if c > batch.min_nz:
+            continue
+        batch.cluster = c
+        for rep in range(2):  # the first run also sets the launch attributes
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, batch.nrve, batch.sys_rve, batch.sys_off,
+                      batch.pcg_status, batch.pcg_iters, batch.pcg_rel, batch.pcg_xnorm)  # fmt: skip
+            end.record()
+            torch.cuda.synchronize()
+        timings[c] = start.elapsed_time(end)
+    batch.cluster = min(timings, key=timings.get) if timings else saved
+    return {"cluster": batch.cluster, "ms": timings}
 
 
 def _timed(timers: dict | None, key: str, fn) -> None:

@@ -278,6 +278,16 @@ int cib_rve_pcg(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve
                 double* Ap, double rtol, int32_t maxit, int32_t* status, int32_t* iterations,
                 double* rel_residual, double* xnorm, void* stream);
 
+/* cib_rve_pcg with `cluster` (1, 2, 4 or 8) CTAs of one thread-block cluster per system:
+ * each CTA owns a slab of z node layers, slab boundaries are exchanged and the dot
+ * products combined through distributed shared memory (fixed rank order, so results are
+ * reproducible for a given cluster size).  Every RVE needs nz >= cluster (else that
+ * system's status is 3); cluster 1 is cib_rve_pcg.  Same reference interface as
+ * cib_rve_pcg (Tᵀ K T + spsolve, src/fem/rve/solver.py:143-144). */
+int cib_rve_pcg_cluster(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve, const int64_t* sys_off,
+                        const int32_t* active, const double* b, const double* dinv, double* x, double* r, double* p,
+                        double* Ap, double rtol, int32_t maxit, int32_t cluster, int32_t* status,
+                        int32_t* iterations, double* rel_residual, double* xnorm, void* stream);
 /* The solve of cib_rve_pcg for callers that cannot allocate device memory -- code running
  * inside an allocator's or memory pool's own hooks, or under a host framework that forbids
  * device allocations after start-up.  No counterpart in the reference (which has no GPU

@@ -1,0 +1,74 @@
+"""GPU tests of the cluster PCG (cib_rve_pcg_cluster): 2, 4 or 8 CTAs of one thread-block
+cluster share each RVE's reduced system; the solution must equal the one-CTA solve up to
+the reordering of its dot products, for uneven batches in both element precisions."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import concrete_impact_b200 as cib
+from concrete_impact_b200 import rve as R
+from concrete_impact_b200.rve_builders import build_two_phase_sphere_rve, config0_materials, default_newton, fp32_newton
+
+pytestmark = pytest.mark.gpu
+
+UPDATE = cib.MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10)
+
+
+def _models(edges, precision):
+    mortar, aggregate = config0_materials()
+    newton = default_newton() if precision == 64 else fp32_newton()
+    return [build_two_phase_sphere_rve((e, e, e), mortar, aggregate, newton, seed=i) for i, e in enumerate(edges)]
+
+
+def _solve(models, precision, cluster, strains, dt=5.0e-6):
+    batch = R.RVEBatch(models, precision=precision, linear_solver=R.LinearSolverOptions(cluster=cluster))
+    batch.macro.copy_(torch.as_tensor(strains, device=batch.device))
+    batch.dt.fill_(dt)
+    res = R.solve_batch_step(batch, models[0].newton_settings, UPDATE, False)
+    batch.response(batch.batch_struct(UPDATE), batch.w, None, None)
+    stress = (batch.sums[:, R.RS_SIGMA : R.RS_SIGMA + 6] / torch.as_tensor(batch.volumes, device=batch.device)[:, None])
+    return stress.cpu().numpy(), res, batch
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-9), (32, 2e-5)])
+def test_cluster_pcg_matches_one_cta(precision: int, tol: float) -> None:
+    edges = [8, 12, 16, 8, 9]
+    models = _models(edges, precision)
+    strains = np.random.default_rng(3).normal(0.0, 1.5e-3, size=(len(edges), 6))
+    ref, res_ref, _ = _solve(models, precision, 1, strains)
+    for cluster in (2, 4, 8):
+        got, res, batch = _solve(models, precision, cluster, strains)
+        assert batch.cluster == cluster
+        scale = np.abs(ref).max(axis=1, keepdims=True)
+        assert np.all(np.abs(got - ref) <= tol * scale), (cluster, np.abs(got - ref).max())
+        assert np.all(np.abs(res.newton_iterations - res_ref.newton_iterations) <= 1)
+        # PCG iteration counts only move by the roundoff of the reordered dot products (in
+        # FP32 the solve ends near the operator's roundoff floor, where counts are sensitive)
+        slack = 2 + 0.02 * res_ref.pcg_iterations if precision == 64 else 10 + 0.15 * res_ref.pcg_iterations
+        assert np.all(np.abs(res.pcg_iterations - res_ref.pcg_iterations) <= slack)
+
+
+def test_cluster_pcg_is_deterministic_and_rejects_thin_rves() -> None:
+    models = _models([8, 12], 64)
+    strains = np.random.default_rng(4).normal(0.0, 1.0e-3, size=(2, 6))
+    a, _, _ = _solve(models, 64, 8, strains)
+    b, _, _ = _solve(models, 64, 8, strains)
+    assert np.array_equal(a, b)
+    with pytest.raises(ValueError, match="element layers"):
+        R.RVEBatch(_models([4], 64), precision=64, linear_solver=R.LinearSolverOptions(cluster=8))
+
+
+def test_auto_and_tuned_cluster_choice() -> None:
+    models = _models([8, 24], 32)
+    batch = R.RVEBatch(models, precision=32, linear_solver=R.LinearSolverOptions(cluster="auto"))
+    assert batch.cluster == 8  # 24^3 = 13,824 elements, smallest nz 8
+    small = R.RVEBatch(_models([8, 8], 32), precision=32, linear_solver=R.LinearSolverOptions(cluster="auto"))
+    assert small.cluster == 1
+    batch.macro.copy_(torch.full((2, 6), 1.0e-3, dtype=torch.float64, device=batch.device))
+    batch.dt.fill_(5.0e-6)
+    out = R.tune_pcg_cluster(batch, UPDATE)
+    assert set(out["ms"]) == {1, 2, 4, 8} and out["cluster"] in out["ms"]
+    assert batch.cluster == out["cluster"]
