@@ -157,7 +157,8 @@ class RNOPoints:
     ``envelope`` = (max |normalised strain|, max |normalised rate|) seen in training, each a
     scalar or a 6-vector of per-component maxima; a point any of whose input components
     exceeds ``envelope_factor`` times its limit is flagged and solved by a fallback RVE from
-    then on (at most ``fallback_capacity`` points).
+    then on (at most ``fallback_capacity`` points).  A point whose surrogate answer is not
+    finite is flagged the same way.
     """
 
     def __init__(self, rno: RNOSurrogate, n_points: int, envelope: tuple[float, float],
@@ -194,6 +195,7 @@ class RNOPoints:
             return stress
         lim_e, lim_r = self._limits(strain.device)
         over = ((strain.abs() / s.strain) > lim_e).any(dim=1) | ((rate.abs() / s.rate) > lim_r).any(dim=1)
+        over |= ~torch.isfinite(stress).all(dim=1) | ~torch.isfinite(strain).all(dim=1)  # never trust a non-finite answer
         new = over & ~self.flagged
         if bool(new.any()):
             self._admit(torch.nonzero(new).flatten(), strain)

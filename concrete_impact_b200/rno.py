@@ -128,6 +128,7 @@ class RNOSurrogate:
         self.step = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.learning_rate = float(config.learning_rate)
+        self.divergences = 0  # epochs rolled back by the training divergence guard
         # fused window kernels (one CTA per 128 paths for the whole window) for width 128
         self.fused = h == 128
         self.skip: torch.Tensor | None = None  # 6x6 normalised elastic skip, fused path only
@@ -354,6 +355,23 @@ class RNOSurrogate:
         return float(w["loss_part"].sum().item()) / float(w["B"] * w["T"] * 6)
 
     # -- training -----------------------------------------------------------------------
+    def _snapshot(self) -> list[torch.Tensor]:
+        """Device copies of the weights, Adam moments and step counter."""
+        out = [self.step.clone()]
+        for L in self.layers:
+            out += [L.w.clone(), L.b.clone(), L.mw.clone(), L.vw.clone(), L.mb.clone(), L.vb.clone()]
+        return out
+
+    def _restore(self, snap: list[torch.Tensor]) -> None:
+        """Copy a snapshot back in place (the captured training graph keeps its buffers)."""
+        self.step.copy_(snap[0])
+        for i, L in enumerate(self.layers):
+            w, b, mw, vw, mb, vb = snap[1 + 6 * i : 7 + 6 * i]
+            for dst, src in ((L.w, w), (L.b, b), (L.mw, mw), (L.vw, vw), (L.mb, mb), (L.vb, vb)):
+                dst.copy_(src)
+            L.wb.copy_(L.w.to(torch.bfloat16))
+            L.wt.copy_(L.w.T.to(torch.bfloat16))
+
     def fit(self, data: RNODataset, epochs: int, graph: bool = True, log=None, lr_schedule=None,
             input_noise: float = 0.0) -> list[float]:  # fmt: skip
         """Train on ``data`` (device-resident); returns the mean loss per epoch.
@@ -376,9 +394,11 @@ class RNOSurrogate:
         gen = torch.Generator(device="cpu").manual_seed(c.seed)
         noise_gen = torch.Generator(device=self.device).manual_seed(c.seed + 1)
         history = []
+        lr_scale = 1.0
+        snapshot = self._snapshot()
         for epoch in range(epochs):
-            if lr_schedule is not None:
-                self.set_learning_rate(lr_schedule(epoch))
+            base = lr_schedule(epoch) if lr_schedule is not None else c.learning_rate
+            self.set_learning_rate(lr_scale * base)
             perm = torch.randperm(P, generator=gen)
             loss_sum = torch.zeros((), dtype=torch.float64, device=self.device)
             windows = 0
@@ -400,6 +420,15 @@ class RNOSurrogate:
                     windows += 1
                     z0 = self._window["z"][W].clone()
             history.append(float(loss_sum.item()) / float(windows * B * W * 6))
+            if not math.isfinite(history[-1]):
+                # divergence guard: back to the last finite epoch, half the step size
+                self._restore(snapshot)
+                lr_scale *= 0.5
+                self.divergences += 1
+                if self.divergences > 8:
+                    raise RuntimeError("surrogate training diverged repeatedly (non-finite loss)")
+            else:
+                snapshot = self._snapshot()
             if log is not None:
                 log(epoch, history[-1])
         if int(self.err.item()) != 0:

@@ -157,6 +157,20 @@ def test_rno_gate_capacity_and_untouched_points() -> None:
         fe2.step()
 
 
+def test_rno_gate_flags_non_finite_answers() -> None:
+    div, lengths = (4, 1, 1), (0.04, 0.01, 0.01)
+    bar = build_macro_bar(div, lengths, 2400.0)
+    dt = stable_time_step(bar, MORTAR.maximum_wave_speed, 0.5)
+    rve = build_structured_rve((2, 2, 2), MORTAR, default_newton())
+    rno = _untrained_rno()
+    rno.layers[3].b.fill_(float("nan"))  # every answer of the surrogate is NaN
+    gated = RNOPoints(rno, bar.points, (1e30, 1e30), rve, SETTINGS, fallback_capacity=bar.points, precision=64)
+    fe2 = ExplicitFE2(bar, gated, dt, _pulse(16 * dt))
+    fe2.run(3)
+    assert gated.slots_used == bar.points
+    assert bool(torch.isfinite(fe2.last_stress).all()) and bool(torch.isfinite(fe2.u).all())
+
+
 def test_generated_paths_of_single_phase_rve_match_point_law() -> None:
     rve = build_structured_rve((2, 2, 2), MORTAR, default_newton())
     spec = PathSetSpec(paths=5, steps=12, seed=31, amplitude=(2e-3, 5e-3), rate_range=(10.0, 1000.0))

@@ -132,6 +132,17 @@ def test_fused_predict_and_rollout_match_unfused() -> None:
     assert _rel(rf.cpu(), rp.cpu()) < 1e-4
 
 
+def test_training_divergence_guard_restores_finite_weights() -> None:
+    data = _material_point_dataset(P=128, T=50, seed=13)
+    scales = RNOScales.from_data(data.strain[:, 1:], data.rates(), data.stress[:, 1:])
+    model = RNOSurrogate(RNOConfig(batch_paths=128, tbptt_steps=50, learning_rate=1.0e30, seed=2), scales)
+    before = [L.w.clone() for L in model.layers]
+    history = model.fit(data, epochs=2)
+    assert model.divergences == 2 and not np.isfinite(history).any()
+    for L, w0 in zip(model.layers, before):  # rolled back to the last finite state
+        assert torch.equal(L.w, w0) and bool(torch.isfinite(L.wb.float()).all())
+
+
 def _material_point_dataset(P: int, T: int, seed: int, dt: float = 2.0e-6) -> RNODataset:
     """Macro stress paths of one viscoplastic mortar point (GPU return map) under random
     piecewise-linear strain paths (|strain| <= 2e-3) with a common time step."""
