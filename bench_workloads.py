@@ -114,7 +114,7 @@ def run_rve_path(args: argparse.Namespace) -> None:
                   "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                                "traffic": None, "peak_kind": kind,
                                "note": "one RVE = one CTA per kernel: latency-bound, not a bandwidth workload"},
-                  "gpu_launches": None,
+                  "gpu_launches": out["launches"],
                   "e2e": {"value": value, "unit": "RVE steps/s", "h2d_bytes_per_step": 6 * 8 * (out["solves"] // out["steps"] + 1),
                           "d2h_bytes_per_step": (6 + 36) * 8 * (out["solves"] // out["steps"] + 1),
                           "path": "solve_rve_microequilibrium (host arrays in and out) in the mixed-control loop"},
@@ -200,7 +200,7 @@ def run_rve_batch(args: argparse.Namespace) -> None:
                                "algorithmic_bytes": pcg_bytes,
                                "note": "algorithmic bytes of all PCG iterations over the PCG launches' event time; "
                                        "small RVEs stay in L2"},
-                  "gpu_launches": sum(out["kernel_launches"].values()),
+                  "gpu_launches": out["launches"],
                   "e2e": {"value": value, "unit": "GP/s", "h2d_bytes_per_step": out["h2d_bytes_per_step"],
                           "d2h_bytes_per_step": out["d2h_bytes_per_step"],
                           "path": "pinned host macro strains -> batched Newton -> pinned host stresses, every step"},
@@ -258,7 +258,7 @@ def run_rno_train(args: argparse.Namespace) -> None:
                                "frac": achieved / peak, "traffic": None, "peak_kind": f"{kind} (cuBLAS bf16, burst)",
                                "kernel": "rno_window_forward/backward + split-K weight-gradient GEMMs",
                                "note": "219,648 FLOP per path-step; the time recursion leaves B/128 CTAs per step"},
-                  "gpu_launches": None,
+                  "gpu_launches": out["launches"],
                   "e2e": {"value": value, "unit": "path-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
                           "path": "device-resident dataset; one loss read-back per epoch"},
                   "clocks": clocks.summary(), "cpu_baseline": None})  # fmt: skip
@@ -331,7 +331,7 @@ def run_fe2(args: argparse.Namespace) -> None:
                   "roofline": {"bound": "tensor", "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
                                "traffic": None, "note": "per step: one fused surrogate launch (T = 1, 1,024 CTAs) "
                                                         "plus the macro Hex8 and Verlet kernels"},
-                  "gpu_launches": None,
+                  "gpu_launches": speed["launches"],
                   "e2e": {"value": value, "unit": "macro steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                           "path": "ExplicitFE2.run on device-resident macro fields"},
                   "clocks": clocks.summary(), "cpu_baseline": None})  # fmt: skip

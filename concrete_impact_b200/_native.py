@@ -246,12 +246,16 @@ def stream_ptr(stream: torch.cuda.Stream | None = None) -> int:
     return stream.cuda_stream
 
 
+LAUNCHED = [0]  # entry-point calls that returned 0 (each launches at most one kernel)
+
+
 def check(code: int, what: str) -> None:
-    """Raise on a non-zero return code of an entry point."""
-    if code != 0:
-        lib = load_library()
-        cuda = lib.cib_last_cuda_error()
-        raise RuntimeError(f"{what} failed with code {code} (last CUDA error {cuda}).")
+    """Raise on a non-zero return code of an entry point; count the successful ones."""
+    if code == 0:
+        LAUNCHED[0] += 1
+        return
+    cuda = load_library().cib_last_cuda_error()
+    raise RuntimeError(f"{what} failed with code {code} (last CUDA error {cuda}).")
 
 
 def j2_diagnostic_names() -> list[str]:

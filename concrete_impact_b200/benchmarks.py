@@ -30,6 +30,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
+from . import _native
 from .materials import MaterialUpdateSettings
 from .rve import (
     RS_SIGMA,
@@ -101,7 +102,9 @@ def rve_path_workload(steps: int = 100) -> dict:
         out["times"] = times
 
     wall0 = time.perf_counter()
+    calls0 = _native.LAUNCHED[0]
     ms = _elapsed_ms(run)
+    out["launches"] = _native.LAUNCHED[0] - calls0
     out.update({"ms": ms, "wall_s": time.perf_counter() - wall0, "steps": steps, "solves": len(solves),
                 "newton_iterations": int(sum(s[0] for s in solves)), "pcg_iterations": int(sum(s[1] for s in solves)),
                 "gauss_points": int(8 * model.elements.shape[0])})  # fmt: skip
@@ -170,7 +173,9 @@ def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision:
         batch.macro.copy_(strain_h[:, warmup + 1])
         batch.dt.copy_(dt_h[:, warmup])
         tuning = tune_pcg_cluster(batch, UPDATE_SETTINGS)
+    calls0 = _native.LAUNCHED[0]
     ms = _elapsed_ms(lambda: [step(t, True) for t in range(warmup + 1, warmup + timed + 1)])
+    launched = _native.LAUNCHED[0] - calls0
     kernel_ms = {k: float(sum(a.elapsed_time(b) for a, b in v)) for k, v in timers.items()}
     launches = {k: len(v) for k, v in timers.items()}
     plastic = float(batch.tflag.float().mean().item())
@@ -178,6 +183,7 @@ def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision:
             "stress_last": stress_h.numpy().copy(), "kernel_ms": kernel_ms, "kernel_launches": launches,
             "plastic_fraction": plastic, "h2d_bytes_per_step": int(batch.nrve * 7 * 8),
             "d2h_bytes_per_step": int(batch.nrve * 6 * 8), "pcg_cluster": int(batch.cluster), "tuning": tuning,
+            "launches": launched,
             **counts}  # fmt: skip
 
 
@@ -221,6 +227,9 @@ def rno_training_workload(paths: int = 2000, steps: int = 200, epochs: int = 300
     out["error_untrained"] = relative_stress_error(rno.rollout(val), target)
     out["error_elastic"] = relative_stress_error(val.strain[:, 1:] @ c_eff.T, target)
     history = rno.fit(data, warmup_epochs)
+    calls0 = _native.LAUNCHED[0]
+    rno.window_step(rno.config.tbptt_steps, min(rno.config.batch_paths, paths))  # eager: count its launches
+    per_window = _native.LAUNCHED[0] - calls0
     c = rno.config
     batch = min(c.batch_paths, paths)
     batches = paths // batch
@@ -229,7 +238,8 @@ def rno_training_workload(paths: int = 2000, steps: int = 200, epochs: int = 300
     out.update({"train_ms": ms, "path_steps": path_steps, "epochs": epochs,
                 "windows": epochs * batches * (steps // c.tbptt_steps), "loss_first": history[0],
                 "loss_last": history[-1], "error_trained": relative_stress_error(rno.rollout(val), target),
-                "flop": path_steps * RNO_TRAIN_FLOP, "model": rno})  # fmt: skip
+                "flop": path_steps * RNO_TRAIN_FLOP, "model": rno,
+                "launches": per_window * epochs * batches * (steps // c.tbptt_steps)})  # fmt: skip
     return out
 
 
@@ -386,8 +396,9 @@ def fe2_speed(rno, envelope, rno_steps: int = 5000, rno_warmup: int = 5, direct_
                 if time.perf_counter() - wall0 > time_limit_s:
                     break
 
+    calls0 = _native.LAUNCHED[0]
     rno_ms = _elapsed_ms(run)
-    out = {"points": bar.points, "dt": dt, "rno_steps": done[0], "rno_steps_requested": rno_steps, "rno_ms": rno_ms,
+    out = {"launches": _native.LAUNCHED[0] - calls0, "points": bar.points, "dt": dt, "rno_steps": done[0], "rno_steps_requested": rno_steps, "rno_ms": rno_ms,
            "rno_steps_per_s": done[0] / (rno_ms / 1e3), "flagged_points": int(gate.slots_used),
            "fallback_steps": int(gate.fallback_steps), "simulated_time_s": (rno_warmup + done[0]) * dt}  # fmt: skip
     del fe2, gate
