@@ -93,9 +93,10 @@ def run_rve_path(args: argparse.Namespace) -> None:
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     from bench import ClockSampler
 
-    rve_path_workload(max(args.warmup, 1))  # warm-up: a short path
+    cluster = int(os.environ.get("CIB_RVE_PATH_CLUSTER", "8"))
+    rve_path_workload(max(args.warmup, 1), cluster)  # warm-up: a short path
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
-        out = rve_path_workload(args.steps)
+        out = rve_path_workload(args.steps, cluster)
     if rank != 0:
         return
     cpu = None if args.no_cpu_baseline else _rve_path_cpu(out)
@@ -106,7 +107,7 @@ def run_rve_path(args: argparse.Namespace) -> None:
     peak, kind = _peak()
     line = _line(args, "accepted RVE steps/s (8^3 concrete RVE, mixed-control uniaxial path, FP64)", value,
                  "RVE steps/s", "rve_path: 8^3 two-phase RVE, seed 0, uniaxial compression -0.5 % in 100 steps at 10/s",
-                 {"ms_per_step": out["ms"] / out["steps"], "dtype": "f64",
+                 {"ms_per_step": out["ms"] / out["steps"], "dtype": "f64", "pcg_cluster": cluster,
                   "gp_evaluations_per_s": out["gp_evaluations"] / seconds,
                   "solves": out["solves"], "newton_iterations": out["newton_iterations"],
                   "pcg_iterations": out["pcg_iterations"],

@@ -34,6 +34,7 @@ from . import _native
 from .materials import MaterialUpdateSettings
 from .rve import (
     RS_SIGMA,
+    LinearSolverOptions,
     RVEBatch,
     StructuredHex8RVE,
     build_rve_operator_cache,
@@ -73,10 +74,11 @@ def _elapsed_ms(fn) -> float:
     return start.elapsed_time(end)
 
 
-def rve_path_workload(steps: int = 100) -> dict:
-    """The mixed-control uniaxial compression path of one 8^3 RVE (FP64)."""
+def rve_path_workload(steps: int = 100, cluster: int = 1) -> dict:
+    """The mixed-control uniaxial compression path of one 8^3 RVE (FP64); ``cluster`` CTAs
+    share its PCG solves."""
     model = concrete_rve(8, 0, 64)
-    cache = build_rve_operator_cache(model)
+    cache = build_rve_operator_cache(model, linear_solver=LinearSolverOptions(cluster=cluster))
     times, exx = uniaxial_path(steps)
     solves: list[tuple[int, int]] = []
     out: dict = {}

@@ -395,10 +395,11 @@ class RNOSurrogate:
         noise_gen = torch.Generator(device=self.device).manual_seed(c.seed + 1)
         history = []
         lr_scale = 1.0
-        snapshot = self._snapshot()
+        good = self._snapshot()  # start of the last epoch whose loss came out finite
         for epoch in range(epochs):
             base = lr_schedule(epoch) if lr_schedule is not None else c.learning_rate
             self.set_learning_rate(lr_scale * base)
+            start = self._snapshot()
             perm = torch.randperm(P, generator=gen)
             loss_sum = torch.zeros((), dtype=torch.float64, device=self.device)
             windows = 0
@@ -420,15 +421,15 @@ class RNOSurrogate:
                     windows += 1
                     z0 = self._window["z"][W].clone()
             history.append(float(loss_sum.item()) / float(windows * B * W * 6))
-            if not math.isfinite(history[-1]):
-                # divergence guard: back to the last finite epoch, half the step size
-                self._restore(snapshot)
+            if math.isfinite(history[-1]):
+                good = start  # every forward pass of this epoch stayed finite
+            else:
+                # divergence guard: back to the start of the last finite epoch, half the step
+                self._restore(good)
                 lr_scale *= 0.5
                 self.divergences += 1
                 if self.divergences > 8:
                     raise RuntimeError("surrogate training diverged repeatedly (non-finite loss)")
-            else:
-                snapshot = self._snapshot()
             if log is not None:
                 log(epoch, history[-1])
         if int(self.err.item()) != 0:

@@ -138,8 +138,10 @@ def test_training_divergence_guard_restores_finite_weights() -> None:
     model = RNOSurrogate(RNOConfig(batch_paths=128, tbptt_steps=50, learning_rate=1.0e30, seed=2), scales)
     before = [L.w.clone() for L in model.layers]
     history = model.fit(data, epochs=2)
-    assert model.divergences == 2 and not np.isfinite(history).any()
-    for L, w0 in zip(model.layers, before):  # rolled back to the last finite state
+    # epoch 1 evaluates the initial weights (finite) and then steps them to ~1e30; epoch 2's
+    # loss overflows, so the guard restores the start of epoch 1
+    assert model.divergences == 1 and np.isfinite(history[0]) and not np.isfinite(history[1])
+    for L, w0 in zip(model.layers, before):
         assert torch.equal(L.w, w0) and bool(torch.isfinite(L.wb.float()).all())
 
 
