@@ -399,7 +399,7 @@ class RNOSurrogate:
         for epoch in range(epochs):
             base = lr_schedule(epoch) if lr_schedule is not None else c.learning_rate
             self.set_learning_rate(lr_scale * base)
-            start = self._snapshot()
+            epoch_start = self._snapshot()
             perm = torch.randperm(P, generator=gen)
             loss_sum = torch.zeros((), dtype=torch.float64, device=self.device)
             windows = 0
@@ -422,7 +422,7 @@ class RNOSurrogate:
                     z0 = self._window["z"][W].clone()
             history.append(float(loss_sum.item()) / float(windows * B * W * 6))
             if math.isfinite(history[-1]):
-                good = start  # every forward pass of this epoch stayed finite
+                good = epoch_start  # every forward pass of this epoch stayed finite
             else:
                 # divergence guard: back to the start of the last finite epoch, half the step
                 self._restore(good)
