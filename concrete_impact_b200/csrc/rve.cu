@@ -649,18 +649,20 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_pcg_kernel(const RvePcgArgs<T
 // closure); after a cluster barrier every rank adds its predecessor's export through
 // distributed shared memory.  Dot products are CTA sums combined over the ranks in rank
 // order (every rank forms the same totals, so all ranks take the same branches).  Four
-// cluster barriers per iteration: export, p.Ap, r.r / r.z, and p visibility.  With C = 1
-// the arithmetic and its order are those of rve_pcg_kernel.
+// cluster barriers per iteration: export, p.Ap, r.r / r.z, and p visibility.  The layer
+// buffers hold the element type T: in FP32 mode the node sums of a layer stay in float
+// (their terms are float element forces), which halves the shared memory, and with at
+// most 128 registers two CTAs fit on an SM.
 template <typename T>
 __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, const double* __restrict__ p,
-                                     double* __restrict__ Ap, double* smem, int k0, int k1,
+                                     double* __restrict__ Ap, T* smem, int k0, int k1,
                                      cg::cluster_group& cl, unsigned prev_rank) {
   const int nxy = d.nx * d.ny;
-  double* ye = smem;                  // nxy * 24
-  double* acc_cur = ye + 24 * nxy;    // nxy * 3
-  double* acc_next = acc_cur + 3 * nxy;
-  double* acc_first = acc_next + 3 * nxy;
-  double* exported = acc_first + 3 * nxy;
+  T* ye = smem;                   // nxy * 24 element-node contributions of one layer
+  T* acc_cur = ye + 24 * nxy;     // nxy * 3 (node sums kept in the element type)
+  T* acc_next = acc_cur + 3 * nxy;
+  T* acc_first = acc_next + 3 * nxy;
+  T* exported = acc_first + 3 * nxy;
   const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
   double pap = 0.0;
   const int items = 8 * nxy;
@@ -705,12 +707,12 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
       reduce_scatter8(f, q, out);
       if (live)
 #pragma unroll
-        for (int dd = 0; dd < 3; ++dd) ye[(8 * el + q) * 3 + dd] = (double)out[dd];
+        for (int dd = 0; dd < 3; ++dd) ye[(8 * el + q) * 3 + dd] = out[dd];
     }
     __syncthreads();
     for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
       const int i = n % d.nx, j = n / d.nx;
-      double bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
+      T bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
       for (int s = 0; s < 4; ++s) {
         const int di = s & 1, dj = s >> 1;
         const int el = (i - di + d.nx) % d.nx + d.nx * ((j - dj + d.ny) % d.ny);
@@ -727,7 +729,7 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
         const int64_t node = d.eoff + n + (int64_t)nxy * k;
 #pragma unroll
         for (int dd = 0; dd < 3; ++dd) {
-          const double v = acc_cur[3 * n + dd] + bot[dd];
+          const double v = (double)(acc_cur[3 * n + dd] + bot[dd]);
           Ap[3 * node + dd] = v;
           pap += p[3 * node + dd] * v;
         }
@@ -741,17 +743,17 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
       }
     }
     __syncthreads();
-    double* t = acc_cur;
+    T* t = acc_cur;
     acc_cur = acc_next;
     acc_next = t;
   }
   cl.sync();  // every rank's export is complete
-  const double* prev = cl.map_shared_rank(exported, prev_rank);
+  const T* prev = cl.map_shared_rank(exported, prev_rank);
   for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
     const int64_t node = d.eoff + n + (int64_t)nxy * k0;
 #pragma unroll
     for (int dd = 0; dd < 3; ++dd) {
-      const double v = (k0 == 0 && n == 0) ? 0.0 : acc_first[3 * n + dd] + prev[3 * n + dd];
+      const double v = (k0 == 0 && n == 0) ? 0.0 : (double)(acc_first[3 * n + dd] + prev[3 * n + dd]);
       Ap[3 * node + dd] = v;
       pap += p[3 * node + dd] * v;
     }
@@ -783,8 +785,9 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NV], double* scratch, do
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RVE_THREADS) rve_pcg_cluster_kernel(const RvePcgArgs<T> a) {
-  extern __shared__ double smem[];
+__global__ void __launch_bounds__(RVE_THREADS, sizeof(T) == 4 ? 2 : 1) rve_pcg_cluster_kernel(const RvePcgArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  T* smem = reinterpret_cast<T*>(smem_bytes);
   __shared__ double scratch[64];
   __shared__ double slot_init[2], slot_pap[1], slot_rr[2], slot_xn[1];
   cg::cluster_group cl = cg::this_cluster();
@@ -1298,7 +1301,7 @@ template <typename T>
 int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cluster, cudaStream_t st) {
   if (cluster == 1) return launch_rve_pcg<T>(a, nsys, max_nxy, st);
   if (cluster != 2 && cluster != 4 && cluster != 8) return CIB_EINVAL;
-  const size_t smem = (size_t)max_nxy * (24 + 12) * sizeof(double);
+  const size_t smem = (size_t)max_nxy * (24 + 12) * sizeof(T);
   if (smem > 200 * 1024) return CIB_ERANGE;
   static bool configured[2] = {false, false};
   const int slot = sizeof(T) == 8 ? 1 : 0;
