@@ -183,7 +183,7 @@ class RNOPoints:
         self.pool_points = torch.full((self.capacity,), -1, dtype=torch.int64, device=dev)
         self.time = 0.0
         self.fallback_steps = 0
-        self.pool_dt_override: tuple[int, int] | None = None
+        self._catch_up: tuple[int, int] | None = None  # slots whose next solve covers the elapsed time
 
     def stress(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
         s = self.rno.scales
@@ -203,11 +203,11 @@ class RNOPoints:
             used = slice(0, self.slots_used)
             pts = self.pool_points[used]
             self.pool.macro[used] = strain[pts]
-            fresh = self.pool_dt_override
             self.pool.dt[used] = dt
-            if fresh is not None:
-                self.pool.dt[fresh[0]:fresh[1]] = max(self.time + dt, dt)
-            self.pool_dt_override = None
+            if self._catch_up is not None:
+                a, b = self._catch_up
+                self.pool.dt[a:b] = max(self.time + dt, dt)
+                self._catch_up = None
             mask = np.zeros(self.capacity, dtype=bool)
             mask[: self.slots_used] = True
             solve_batch_step(self.pool, self.model.newton_settings, self.settings, False, live_mask=mask)
@@ -244,7 +244,7 @@ class RNOPoints:
         p.w_n[3 * E * a : 3 * E * b] = 0
         p.macro_n[a:b] = 0
         self.slots_used = b
-        self.pool_dt_override = (a, b)
+        self._catch_up = (a, b) if self._catch_up is None else (self._catch_up[0], b)
 
     def commit(self) -> None:
         self.z = self.z_next.clone()
