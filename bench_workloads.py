@@ -227,6 +227,41 @@ def _tensor_peak() -> tuple[float, str]:
     return 1590.0, "fallback"
 
 
+def _rno_train_cpu(windows: int = 6) -> dict:
+    """The training loop in torch on the host (the reference's way of training its
+    surrogate), same network, batch 512, TBPTT 50, float32, all host threads."""
+    import torch
+
+    from oracle.rno_torch import train_windows
+
+    g = torch.Generator().manual_seed(0)
+    shape = (600, 200, 6)
+    out = train_windows(torch.randn(shape, generator=g), torch.randn(shape, generator=g), torch.randn(shape, generator=g),
+                        torch.rand(shape[:2], generator=g) * 0.1, windows=windows)  # fmt: skip
+    return {"value": out["path_steps"] / out["seconds"], "unit": "path-steps/s", "cores": out["threads"], "kind": "port",
+            "sample": f"{windows} TBPTT windows of 512 paths x 50 steps, torch float32 autograd + Adam on the host "
+                      "(oracle/rno_torch.py)"}  # fmt: skip
+
+
+def _fe2_cpu(solves: int = 3) -> dict:
+    """Direct FE^2 on the host: the oracle's 8^3 RVE solve (the reference's algorithm, FP64
+    direct sparse solves) timed per solve; one solve per macro point per step, spread over
+    all host cores without loss (which favours the CPU)."""
+    from concrete_impact_b200.benchmarks import concrete_rve
+
+    oracle = _oracle_for(concrete_rve(8, 0, 64), 1.0e-8)
+    state = oracle.initial_state()
+    t0 = time.perf_counter()
+    for k in range(1, solves + 1):
+        macro = np.array([-1.0e-3, 2.0e-4, 2.0e-4, 0.0, 0.0, 0.0]) * k / solves
+        state = oracle.solve(macro, 1.0e-6, state, False)["state"]
+    per_solve = (time.perf_counter() - t0) / solves
+    cores = os.cpu_count() or 1
+    return {"value": cores / (131072 * per_solve), "unit": "macro steps/s", "cores": cores, "kind": "port",
+            "sample": f"oracle 8^3 RVE solves ({per_solve:.3f} s each, {solves} loading steps) x 131,072 macro points "
+                      f"per step / {cores} cores"}  # fmt: skip
+
+
 def run_rno_train(args: argparse.Namespace) -> None:
     import torch
 
@@ -262,7 +297,7 @@ def run_rno_train(args: argparse.Namespace) -> None:
                   "gpu_launches": out["launches"],
                   "e2e": {"value": value, "unit": "path-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
                           "path": "device-resident dataset; one loss read-back per epoch"},
-                  "clocks": clocks.summary(), "cpu_baseline": None})  # fmt: skip
+                  "clocks": clocks.summary(), "cpu_baseline": None if args.no_cpu_baseline else _rno_train_cpu()})  # fmt: skip
     print(json.dumps(line), flush=True)
 
 
@@ -335,13 +370,25 @@ def run_fe2(args: argparse.Namespace) -> None:
                   "gpu_launches": speed["launches"],
                   "e2e": {"value": value, "unit": "macro steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                           "path": "ExplicitFE2.run on device-resident macro fields"},
-                  "clocks": clocks.summary(), "cpu_baseline": None})  # fmt: skip
+                  "clocks": clocks.summary(), "cpu_baseline": None if args.no_cpu_baseline else _fe2_cpu()})  # fmt: skip
     print(json.dumps(line), flush=True)
 
 
 def run_reference(args: argparse.Namespace) -> None:
     """``--impl reference``: the oracle alone on the workload's CPU sample (rank 0)."""
     if int(os.environ.get("RANK", "0")) != 0:
+        return
+    if args.workload in ("rno_train", "fe2"):
+        c = _rno_train_cpu() if args.workload == "rno_train" else _fe2_cpu()
+        value, unit, sample = c["value"], c["unit"], c["sample"]
+        metric = ("surrogate training throughput (torch on the host)" if args.workload == "rno_train"
+                  else "direct FE2 macro steps/s (oracle RVE solves on the host)")  # fmt: skip
+        line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32" if args.workload == "rno_train" else "f64", "data": "synthetic",
+                "config": {"workload": args.workload}, "cpu_baseline": c,
+                "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}  # fmt: skip
+        print(json.dumps(line), flush=True)
         return
     if args.workload == "rve_batch":
         from concrete_impact_b200.benchmarks import concrete_rve
