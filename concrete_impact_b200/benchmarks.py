@@ -256,13 +256,13 @@ class FE2Recipe:
     from direct FE^2 runs of a calibration bar at other pulse amplitudes (the reference's
     impact_path data source)."""
 
-    random_paths: int = 2000
+    random_paths: int = 1000
     random_amplitude: tuple[float, float] = (2.0e-4, 5.0e-3)
     path_steps: int = 400
     impact_amplitudes: tuple[float, ...] = (20.0e6, 30.0e6, 40.0e6, 60.0e6, 70.0e6, 80.0e6)
     calibration_divisions: tuple[int, int, int] = (64, 2, 2)
     point_stride: int = 2
-    epochs: int = 1500
+    epochs: int = 2500
     tau_ref: float = 1.0e-4
     learning_rate: float = 1.0e-3
     final_lr_fraction: float = 0.02
