@@ -649,20 +649,20 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_pcg_kernel(const RvePcgArgs<T
 // closure); after a cluster barrier every rank adds its predecessor's export through
 // distributed shared memory.  Dot products are CTA sums combined over the ranks in rank
 // order (every rank forms the same totals, so all ranks take the same branches).  Four
-// cluster barriers per iteration: export, p.Ap, r.r / r.z, and p visibility.  The layer
-// buffers hold the element type T: in FP32 mode the node sums of a layer stay in float
-// (their terms are float element forces), which halves the shared memory, and with at
-// most 128 registers two CTAs fit on an SM.
+// cluster barriers per iteration: export, p.Ap, r.r / r.z, and p visibility.  The layer's
+// element contributions are kept in the element type T (exact: they are computed in T),
+// the node sums in double as in rve_pcg_kernel; in FP32 mode that is 192 bytes per node of
+// a layer, and with at most 128 registers two CTAs fit on an SM.
 template <typename T>
 __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, const double* __restrict__ p,
-                                     double* __restrict__ Ap, T* smem, int k0, int k1,
+                                     double* __restrict__ Ap, unsigned char* smem, int k0, int k1,
                                      cg::cluster_group& cl, unsigned prev_rank) {
   const int nxy = d.nx * d.ny;
-  T* ye = smem;                   // nxy * 24 element-node contributions of one layer
-  T* acc_cur = ye + 24 * nxy;     // nxy * 3 (node sums kept in the element type)
-  T* acc_next = acc_cur + 3 * nxy;
-  T* acc_first = acc_next + 3 * nxy;
-  T* exported = acc_first + 3 * nxy;
+  T* ye = reinterpret_cast<T*>(smem);  // nxy * 24 element-node contributions of one layer (exact in T)
+  double* acc_cur = reinterpret_cast<double*>(smem + (size_t)24 * nxy * sizeof(T));  // nxy * 3 node sums
+  double* acc_next = acc_cur + 3 * nxy;
+  double* acc_first = acc_next + 3 * nxy;
+  double* exported = acc_first + 3 * nxy;
   const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
   double pap = 0.0;
   const int items = 8 * nxy;
@@ -712,14 +712,14 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
     __syncthreads();
     for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
       const int i = n % d.nx, j = n / d.nx;
-      T bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
+      double bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
       for (int s = 0; s < 4; ++s) {
         const int di = s & 1, dj = s >> 1;
         const int el = (i - di + d.nx) % d.nx + d.nx * ((j - dj + d.ny) % d.ny);
 #pragma unroll
         for (int dd = 0; dd < 3; ++dd) {
-          bot[dd] += ye[(8 * el + s) * 3 + dd];
-          top[dd] += ye[(8 * el + s + 4) * 3 + dd];
+          bot[dd] += (double)ye[(8 * el + s) * 3 + dd];
+          top[dd] += (double)ye[(8 * el + s + 4) * 3 + dd];
         }
       }
       if (k == k0) {
@@ -729,7 +729,7 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
         const int64_t node = d.eoff + n + (int64_t)nxy * k;
 #pragma unroll
         for (int dd = 0; dd < 3; ++dd) {
-          const double v = (double)(acc_cur[3 * n + dd] + bot[dd]);
+          const double v = acc_cur[3 * n + dd] + bot[dd];
           Ap[3 * node + dd] = v;
           pap += p[3 * node + dd] * v;
         }
@@ -743,17 +743,17 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
       }
     }
     __syncthreads();
-    T* t = acc_cur;
+    double* t = acc_cur;
     acc_cur = acc_next;
     acc_next = t;
   }
   cl.sync();  // every rank's export is complete
-  const T* prev = cl.map_shared_rank(exported, prev_rank);
+  const double* prev = cl.map_shared_rank(exported, prev_rank);
   for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
     const int64_t node = d.eoff + n + (int64_t)nxy * k0;
 #pragma unroll
     for (int dd = 0; dd < 3; ++dd) {
-      const double v = (k0 == 0 && n == 0) ? 0.0 : (double)(acc_first[3 * n + dd] + prev[3 * n + dd]);
+      const double v = (k0 == 0 && n == 0) ? 0.0 : acc_first[3 * n + dd] + prev[3 * n + dd];
       Ap[3 * node + dd] = v;
       pap += p[3 * node + dd] * v;
     }
@@ -786,8 +786,8 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NV], double* scratch, do
 
 template <typename T>
 __global__ void __launch_bounds__(RVE_THREADS, sizeof(T) == 4 ? 2 : 1) rve_pcg_cluster_kernel(const RvePcgArgs<T> a) {
-  extern __shared__ __align__(16) unsigned char smem_bytes[];
-  T* smem = reinterpret_cast<T*>(smem_bytes);
+  extern __shared__ double smem_dyn[];  // the layer buffers of apply_tangent_slab
+  unsigned char* smem = reinterpret_cast<unsigned char*>(smem_dyn);
   __shared__ double scratch[64];
   __shared__ double slot_init[2], slot_pap[1], slot_rr[2], slot_xn[1];
   cg::cluster_group cl = cg::this_cluster();
@@ -1301,7 +1301,7 @@ template <typename T>
 int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cluster, cudaStream_t st) {
   if (cluster == 1) return launch_rve_pcg<T>(a, nsys, max_nxy, st);
   if (cluster != 2 && cluster != 4 && cluster != 8) return CIB_EINVAL;
-  const size_t smem = (size_t)max_nxy * (24 + 12) * sizeof(T);
+  const size_t smem = (size_t)max_nxy * (24 * sizeof(T) + 12 * sizeof(double));
   if (smem > 200 * 1024) return CIB_ERANGE;
   static bool configured[2] = {false, false};
   const int slot = sizeof(T) == 8 ? 1 : 0;
