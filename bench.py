@@ -10,9 +10,12 @@ tangent=True).  Headline precision is float64 (the reference's); the float32 var
 the method is reported alongside.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload return_map|rve_path|rve_batch|rno_train|fe2]
 
 Under torchrun each rank updates its own batch of the same size (independent points:
-weak scaling, no collective on the data path); rank 0 prints the line.
+weak scaling, no collective on the data path); rank 0 prints the line.  The other
+workloads (the RVE path, the 256-RVE batch, surrogate training and FE^2) are in
+bench_workloads.py.
 """
 
 from __future__ import annotations
@@ -237,6 +240,17 @@ def cpu_baseline_c(n_sample: int) -> dict:
     }
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest of every rank's value (one all-reduce; ``dist`` None = one process)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args: argparse.Namespace) -> None:
     import numpy as np
     import torch
@@ -350,11 +364,7 @@ def run_ours(args: argparse.Namespace) -> None:
     e2e_s, h2d_b, d2h_b, e2e_fail, e2e_launches = e2e_timed(torch.float64)
 
     def reduce_max(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, dist, dev)
 
     total64 = reduce_max(total64)
     total32 = reduce_max(total32)
