@@ -134,21 +134,48 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
   double sq = 0.0;
   uint32_t phase = 0;
   bool ok = true;
+  // inputs of the next step, loaded one step ahead so that their latency hides behind
+  // the current step's layers
+  float ne[6] = {0, 0, 0, 0, 0, 0}, nr[6] = {0, 0, 0, 0, 0, 0}, nt[6] = {0, 0, 0, 0, 0, 0}, nc = 0.0f;
+  if (half == 0 && valid) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      ne[k] = w.strain[(size_t)p * 6 + k];
+      nr[k] = w.rate[(size_t)p * 6 + k];
+      if (w.target) nt[k] = w.target[(size_t)p * 6 + k];
+    }
+    nc = w.coef[p];
+  }
   for (int t = 0; t < T && ok; ++t) {
     const size_t g = (size_t)t * B + p;  // (t, p) row of the window
-    float e[6] = {0, 0, 0, 0, 0, 0};
+    float e[6], tg[6];
+    const float c = nc;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      e[k] = ne[k];
+      tg[k] = nt[k];
+    }
     if (half == 0) {
       float xin[XIN];
 #pragma unroll
-      for (int c = 0; c < XIN; ++c) xin[c] = 0.0f;
+      for (int c2 = 0; c2 < XIN; ++c2) xin[c2] = 0.0f;
       if (valid) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-          e[k] = w.strain[g * 6 + k];
           xin[k] = e[k];
-          xin[6 + k] = w.rate[g * 6 + k];
+          xin[6 + k] = nr[k];
           xin[12 + k] = z[k];
         }
+      }
+      if (valid && t + 1 < T) {
+        const size_t gn = g + (size_t)B;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          ne[k] = w.strain[gn * 6 + k];
+          nr[k] = w.rate[gn * 6 + k];
+          if (w.target) nt[k] = w.target[gn * 6 + k];
+        }
+        nc = w.coef[gn];
       }
 #pragma unroll
       for (int c = 0; c < XIN; c += 8) put8(S.x, row, c, XIN, xin + c);
@@ -194,7 +221,6 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
       float v[16];
       tmem_ld16(lane_addr, v);
       if (valid) {
-        const float c = w.coef[g];
         float s[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) s[k] = v[k] + S.bias[3 * HID + k];
@@ -213,7 +239,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
         if (w.target) {
 #pragma unroll
           for (int k = 0; k < 6; ++k) {
-            const float d = s[k] - w.target[g * 6 + k];
+            const float d = s[k] - tg[k];
             sq += (double)d * d;
             if (w.gS) w.gS[g * 6 + k] = w.loss_scale * 2.0f * d;
           }
@@ -279,20 +305,35 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
   float dz[6] = {0, 0, 0, 0, 0, 0};
   uint32_t phase = 0;
   bool ok = true;
+  // loss gradient and coefficient of the next (earlier) step, loaded one step ahead
+  float ng[6] = {0, 0, 0, 0, 0, 0}, ncf = 0.0f;
+  if (half == 0 && valid) {
+    const size_t gl = (size_t)(T - 1) * B + p;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ng[k] = w.gS[gl * 6 + k];
+    ncf = w.coef[gl];
+  }
   for (int t = T - 1; t >= 0 && ok; --t) {
     const size_t g = (size_t)t * B + p;
-    float gs[6] = {0, 0, 0, 0, 0, 0};
+    float gs[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) gs[k] = ng[k];
+    const float cf = ncf;
     if (half == 0) {
       float dy[YOUT];
 #pragma unroll
       for (int c = 0; c < YOUT; ++c) dy[c] = 0.0f;
       if (valid) {
-        const float c = w.coef[g];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-          gs[k] = w.gS[g * 6 + k];
           dy[k] = gs[k];
-          dy[6 + k] = c * dz[k];
+          dy[6 + k] = cf * dz[k];
+        }
+        if (t > 0) {
+          const size_t gp = g - (size_t)B;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) ng[k] = w.gS[gp * 6 + k];
+          ncf = w.coef[gp];
         }
 #pragma unroll
         for (int c2 = 0; c2 < YOUT; ++c2) dYt[(size_t)c2 * R + g] = __float2bfloat16_rn(dy[c2]);
