@@ -14,8 +14,10 @@
   metric: macro steps/s, with all-direct FE^2 timed beside it and the surrogate's error
   against all-direct FP64 FE^2 on a 64x2x2 bar.
 
-The CPU baseline of both is the NumPy/SciPy oracle of the reference's RVE solve (direct
-sparse solves, the reference's algorithm) timed on the host on a bounded sample.
+CPU baselines, each timed on the host on a bounded sample: the NumPy/SciPy oracle of the
+reference's RVE solve (direct sparse solves, the reference's algorithm) for rve_path,
+rve_batch and fe2, and the torch training loop on the host (oracle/rno_torch.py) for
+rno_train.
 Multi-GPU runs are replicas: every rank runs the same workload, rank 0 prints.
 """
 
@@ -102,8 +104,8 @@ def run_rve_path(args: argparse.Namespace) -> None:
     cpu = None if args.no_cpu_baseline else _rve_path_cpu(out)
     seconds = out["ms"] / 1e3
     value = out["steps"] / seconds
-    # dominant work: the Newton residual passes (984 algorithmic bytes per element, FP64
-    # element state counted at 8 bytes) -- one CTA per system, so the fraction is small
+    # one 8^3 RVE occupies at most one cluster of CTAs: a latency-bound solve, not a
+    # bandwidth workload, so no roofline fraction is claimed
     peak, kind = _peak()
     line = _line(args, "accepted RVE steps/s (8^3 concrete RVE, mixed-control uniaxial path, FP64)", value,
                  "RVE steps/s", "rve_path: 8^3 two-phase RVE, seed 0, uniaxial compression -0.5 % in 100 steps at 10/s",
@@ -114,7 +116,7 @@ def run_rve_path(args: argparse.Namespace) -> None:
                   "final_macro_stress_xx_pa": float(out["macro_stress"][-1][0]),
                   "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                                "traffic": None, "peak_kind": kind,
-                               "note": "one RVE = one CTA per kernel: latency-bound, not a bandwidth workload"},
+                               "note": "one RVE = one CTA or one cluster per kernel: latency-bound, not a bandwidth workload"},
                   "gpu_launches": out["launches"],
                   "e2e": {"value": value, "unit": "RVE steps/s", "h2d_bytes_per_step": 6 * 8 * (out["solves"] // out["steps"] + 1),
                           "d2h_bytes_per_step": (6 + 36) * 8 * (out["solves"] // out["steps"] + 1),
