@@ -190,6 +190,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_counter_increment": (_I, [_P, _P]),
     "cib_rno_window_forward": (_I, [_P, _P]),
     "cib_rno_window_backward": (_I, [_P, _P]),
+    "cib_rno_gate_prepare": (_I, [_I64, _P, _P, _D, _D, _P, _D] + [_P] * 7),
+    "cib_rno_gate_finish": (_I, [_I64, _P, _D, _P, _P, _P, _P, _P]),
     "cib_verlet_predict": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P]),
     "cib_verlet_correct": (_I, [_I64, _P, _D, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     "cib_rve_residual": (_I, [_P] * 9),

@@ -184,8 +184,22 @@ class RNOPoints:
         self.time = 0.0
         self.fallback_steps = 0
         self._catch_up: tuple[int, int] | None = None  # slots whose next solve covers the elapsed time
+        self.lib = _native.load_library()
+        if rno.fused:  # device buffers of the fused gate (two launches around the surrogate per step)
+            f32 = torch.float32
+            self.zbuf = torch.zeros((2, n_points, 6), dtype=f32, device=dev)  # current / next latent
+            self.xn = torch.empty((n_points, 6), dtype=f32, device=dev)
+            self.rn = torch.empty((n_points, 6), dtype=f32, device=dev)
+            self.cf = torch.empty(n_points, dtype=f32, device=dev)
+            self.sn = torch.empty((n_points, 6), dtype=f32, device=dev)
+            self.out = torch.empty((n_points, 6), dtype=torch.float64, device=dev)
+            self.fresh = torch.zeros(n_points, dtype=torch.uint8, device=dev)
+            self.flag8 = torch.zeros(n_points, dtype=torch.uint8, device=dev)
+            self.count = torch.zeros(1, dtype=torch.int32, device=dev)
 
     def stress(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
+        if self.rno.fused and self.pool is not None:
+            return self._stress_fused(strain, rate, dt)
         s = self.rno.scales
         coef = torch.full((self.n,), dt / self.rno.config.tau_ref, dtype=torch.float32, device=strain.device)
         out, z_next, self.buffers = self.rno.predict(strain, rate, self.z, coef, self.buffers)
@@ -200,21 +214,54 @@ class RNOPoints:
         if bool(new.any()):
             self._admit(torch.nonzero(new).flatten(), strain)
         if self.slots_used:
-            used = slice(0, self.slots_used)
-            pts = self.pool_points[used]
-            self.pool.macro[used] = strain[pts]
-            self.pool.dt[used] = dt
-            if self._catch_up is not None:
-                a, b = self._catch_up
-                self.pool.dt[a:b] = max(self.time + dt, dt)
-                self._catch_up = None
-            mask = np.zeros(self.capacity, dtype=bool)
-            mask[: self.slots_used] = True
-            solve_batch_step(self.pool, self.model.newton_settings, self.settings, False, live_mask=mask)
-            self.pool.response(self.pool.batch_struct(self.settings), self.pool.w, None, None)
-            vol = float(self.pool.volumes[0])
-            stress[pts] = self.pool.sums[used, RS_SIGMA : RS_SIGMA + 6] / vol
-            self.fallback_steps += 1
+            self._solve_pool(stress, strain, dt)
+        return stress
+
+    def _solve_pool(self, stress: torch.Tensor, strain: torch.Tensor, dt: float) -> None:
+        """Direct RVE solves of the flagged points; their rows of ``stress`` are replaced."""
+        used = slice(0, self.slots_used)
+        pts = self.pool_points[used]
+        self.pool.macro[used] = strain[pts]
+        self.pool.dt[used] = dt
+        if self._catch_up is not None:
+            a, b = self._catch_up
+            self.pool.dt[a:b] = max(self.time + dt, dt)
+            self._catch_up = None
+        mask = np.zeros(self.capacity, dtype=bool)
+        mask[: self.slots_used] = True
+        solve_batch_step(self.pool, self.model.newton_settings, self.settings, False, live_mask=mask)
+        self.pool.response(self.pool.batch_struct(self.settings), self.pool.w, None, None)
+        vol = float(self.pool.volumes[0])
+        stress[pts] = self.pool.sums[used, RS_SIGMA : RS_SIGMA + 6] / vol
+        self.fallback_steps += 1
+
+    def _stress_fused(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
+        """The gate in two kernels around the fused surrogate step: normalise and test the
+        inputs, run the surrogate, scale and test its answers; one read of the count of
+        newly flagged points decides whether the fallback pool is needed."""
+        s = self.rno.scales
+        lim_e, lim_r = self._limits(strain.device)
+        if not hasattr(self, "_lim12"):
+            self._lim12 = torch.cat([lim_e.expand(6), lim_r.expand(6)]).contiguous()
+        strain, rate = strain.contiguous(), rate.contiguous()
+        sp = _native.stream_ptr()
+        self.count.zero_()
+        _native.check(self.lib.cib_rno_gate_prepare(
+            self.n, strain.data_ptr(), rate.data_ptr(), s.strain, s.rate, self._lim12.data_ptr(),
+            dt / self.rno.config.tau_ref, self.flag8.data_ptr(), self.xn.data_ptr(), self.rn.data_ptr(),
+            self.cf.data_ptr(), self.fresh.data_ptr(), self.count.data_ptr(), sp), "cib_rno_gate_prepare")  # fmt: skip
+        self.rno.predict_normalized(self.xn, self.rn, self.cf, self.zbuf, self.sn)
+        _native.check(self.lib.cib_rno_gate_finish(
+            self.n, self.sn.data_ptr(), s.stress, self.flag8.data_ptr(), self.fresh.data_ptr(), self.count.data_ptr(),
+            self.out.data_ptr(), sp), "cib_rno_gate_finish")  # fmt: skip
+        stress = self.out
+        if int(self.count.item()) > 0:
+            new = torch.nonzero(self.fresh).flatten()
+            self.flag8[new] = 1
+            self._admit(new, strain)
+        if self.slots_used:
+            stress = stress.clone()
+            self._solve_pool(stress, strain, dt)
         return stress
 
     def _limits(self, device) -> tuple[torch.Tensor, torch.Tensor]:
@@ -247,7 +294,10 @@ class RNOPoints:
         self._catch_up = (a, b) if self._catch_up is None else (self._catch_up[0], b)
 
     def commit(self) -> None:
-        self.z = self.z_next.clone()
+        if self.rno.fused and self.pool is not None:
+            self.zbuf[0].copy_(self.zbuf[1])
+        else:
+            self.z = self.z_next.clone()
         if self.slots_used:
             self.pool.commit()
 

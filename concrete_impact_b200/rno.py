@@ -497,6 +497,23 @@ class RNOSurrogate:
         _check(self.lib.cib_rno_window_forward(ctypes.byref(c), _native.stream_ptr()), "cib_rno_window_forward")
         return buffers["stress"][0] * s.stress, buffers["z"][1], buffers
 
+    def predict_normalized(self, strain_n: torch.Tensor, rate_n: torch.Tensor, coef: torch.Tensor, z: torch.Tensor,
+                           stress_n: torch.Tensor) -> None:  # fmt: skip
+        """One fused step on prepared inputs: normalised fp32 strain and rate (M, 6), coef
+        (M,), latent buffer z (2, M, 6) with the current latent in z[0] (z[1] receives the
+        next), normalised stress out (M, 6).  Fused kernels only (hidden width 128)."""
+        if not self.fused:
+            raise ValueError("predict_normalized needs the fused kernels (hidden width 128)")
+        c = _native.RNOWindowC()
+        c.B, c.T, c.hidden = int(strain_n.shape[0]), 1, self.config.hidden
+        c.strain, c.rate, c.coef, c.z = strain_n.data_ptr(), rate_n.data_ptr(), coef.data_ptr(), z.data_ptr()
+        for i, L in enumerate(self.layers):
+            c.W[i], c.bias[i] = L.wb.data_ptr(), L.b.data_ptr()
+        c.skip = None if self.skip is None else self.skip.data_ptr()
+        c.stress = stress_n.data_ptr()
+        c.err = self.err.data_ptr()
+        _check(self.lib.cib_rno_window_forward(ctypes.byref(c), _native.stream_ptr()), "cib_rno_window_forward")
+
     def _predict_unfused(self, strain, rate, z, coef, buffers):
         M = int(strain.shape[0])
         dev, h = self.device, self.config.hidden

@@ -427,6 +427,20 @@ int cib_verlet_correct(int64_t n, const double* f_unit, double load_scale, const
                        const uint8_t* fixed, double dt, const double* a, const double* v, double* a_next,
                        double* v_next, void* stream);
 
+/* Error gate of the surrogate at n macro points (no reference counterpart; the reference's
+ * deployment adapter, src/concrete_impact/nn/deployment.py:68-165, has no input gate).
+ * prepare: strain_n = strain / strain_scale, rate_n = rate / rate_scale (fp32, n x 6),
+ * coef_out[i] = coef, and fresh[i] = 1 for each point not yet `flagged` whose strain or rate
+ * component exceeds limits[0..5] / limits[6..11] (normalised units) or is not finite;
+ * finish: stress = stress_n * stress_scale (double) and fresh[i] = 1 also where the
+ * surrogate's answer is not finite.  Both add the number of newly set `fresh` points to
+ * the device counter `count`. */
+int cib_rno_gate_prepare(int64_t n, const double* strain, const double* rate, double strain_scale, double rate_scale,
+                         const double* limits, double coef, const uint8_t* flagged, float* strain_n, float* rate_n,
+                         float* coef_out, uint8_t* fresh, unsigned int* count, void* stream);
+int cib_rno_gate_finish(int64_t n, const float* stress_n, double stress_scale, const uint8_t* flagged, uint8_t* fresh,
+                        unsigned int* count, double* stress, void* stream);
+
 /* Strided host<->device copy of `rows` rows of `row_bytes` bytes (one cudaMemcpy2DAsync);
  * kind 1 = host to device, 2 = device to host, 3 = device to device. */
 int cib_copy_rows_async(void* dst, int64_t dst_pitch, const void* src, int64_t src_pitch, int64_t row_bytes,

@@ -157,6 +157,40 @@ def test_rno_gate_capacity_and_untouched_points() -> None:
         fe2.step()
 
 
+def test_gate_kernels_match_formula() -> None:
+    lib = _native.load_library()
+    g = torch.Generator(device="cuda").manual_seed(4)
+    n = 1000
+    strain = torch.randn((n, 6), generator=g, device="cuda", dtype=torch.float64) * 1e-3
+    rate = torch.randn((n, 6), generator=g, device="cuda", dtype=torch.float64) * 50.0
+    strain[7, 2] = float("nan")
+    lim = torch.tensor([2.0] * 6 + [2.5] * 6, dtype=torch.float64, device="cuda")
+    flagged = (torch.rand(n, generator=g, device="cuda") < 0.2).to(torch.uint8)
+    xn, rn, sn = (torch.empty((n, 6), dtype=torch.float32, device="cuda") for _ in range(3))
+    cf = torch.empty(n, dtype=torch.float32, device="cuda")
+    fresh = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = torch.empty((n, 6), dtype=torch.float64, device="cuda")
+    sp = _native.stream_ptr()
+    _native.check(lib.cib_rno_gate_prepare(n, strain.data_ptr(), rate.data_ptr(), 1e-3, 40.0, lim.data_ptr(), 0.25,
+                                           flagged.data_ptr(), xn.data_ptr(), rn.data_ptr(), cf.data_ptr(),
+                                           fresh.data_ptr(), count.data_ptr(), sp), "prepare")  # fmt: skip
+    en, rnr = strain / 1e-3, rate / 40.0
+    over = ~((en.abs() <= 2.0).all(1) & (rnr.abs() <= 2.5).all(1))
+    expect = over & (flagged == 0)
+    assert torch.equal(fresh.bool(), expect) and int(count.item()) == int(expect.sum())
+    torch.testing.assert_close(rn, rnr.float())
+    assert bool((cf == 0.25).all())
+    sn.copy_(torch.randn((n, 6), generator=g, device="cuda"))
+    sn[11, 0] = float("inf")
+    before = fresh.clone()
+    _native.check(lib.cib_rno_gate_finish(n, sn.data_ptr(), 2.0e7, flagged.data_ptr(), fresh.data_ptr(),
+                                          count.data_ptr(), out.data_ptr(), sp), "finish")  # fmt: skip
+    torch.testing.assert_close(out[:11], sn[:11].double() * 2.0e7)
+    extra = int((~before.bool() & (flagged == 0))[11])
+    assert bool(fresh[11]) == bool(flagged[11] == 0) and int(count.item()) == int(expect.sum()) + extra
+
+
 def test_rno_gate_flags_non_finite_answers() -> None:
     div, lengths = (4, 1, 1), (0.04, 0.01, 0.01)
     bar = build_macro_bar(div, lengths, 2400.0)
