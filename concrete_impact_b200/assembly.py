@@ -15,7 +15,6 @@ the kernels of ``csrc/hex8.cu`` with a deterministic (fixed-order, atomic-free) 
 
 from __future__ import annotations
 
-import ctypes
 from dataclasses import dataclass, field
 from typing import Any
 

@@ -28,7 +28,7 @@ from . import _native
 from .assembly import MaterialAssemblyCache, build_hex8_material_assembly_cache
 from .materials import MaterialPointRequest, MaterialState, MaterialUpdateSettings
 from .rno import RNOSurrogate
-from .rve import RS_SIGMA, NonlinearNewtonSettings, RVEBatch, StructuredHex8RVE, build_structured_hex8_box, solve_batch_step
+from .rve import RS_SIGMA, RVEBatch, StructuredHex8RVE, build_structured_hex8_box, solve_batch_step
 
 
 @dataclass

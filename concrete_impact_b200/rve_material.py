@@ -45,7 +45,6 @@ from .rve import (
     StructuredHex8RVE,
     _phase_points,
     _phases_of,
-    build_rve_operator_cache,
     initialize_rve_state,
     solve_batch_step,
 )
