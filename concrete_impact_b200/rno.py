@@ -167,6 +167,28 @@ class RNOSurrogate:
         self._structs = {}
         self._graph = None
 
+    def checkpoint(self) -> dict[str, torch.Tensor]:
+        """Weights, scales, skip term, Adam moments, step counter and step size (host
+        tensors): everything training needs to resume, as the reference's training loop
+        checkpoints model and optimizer together (src/concrete_impact/nn/training/rve_rno.py:997-1012)."""
+        out = self.state_dict()
+        out["tau_ref"] = torch.tensor(self.config.tau_ref, dtype=torch.float64)
+        out["learning_rate"] = torch.tensor(self.learning_rate, dtype=torch.float64)
+        out["adam.step"] = self.step.detach().cpu().clone()
+        for i, L in enumerate(self.layers):
+            for name in ("mw", "vw", "mb", "vb"):
+                out[f"adam.{i}.{name}"] = getattr(L, name).detach().cpu().clone()
+        return out
+
+    def load_checkpoint(self, state: dict[str, torch.Tensor]) -> None:
+        """Restore a ``checkpoint``; training continues where it stopped."""
+        self.load_state_dict(state)
+        self.step.copy_(state["adam.step"].to(self.device))
+        for i, L in enumerate(self.layers):
+            for name in ("mw", "vw", "mb", "vb"):
+                getattr(L, name).copy_(state[f"adam.{i}.{name}"].to(self.device))
+        self.set_learning_rate(float(state["learning_rate"]))
+
     # -- window buffers ---------------------------------------------------------------
     def _buffers(self, T: int, B: int) -> dict:
         if self._window is not None and self._window["T"] == T and self._window["B"] == B:

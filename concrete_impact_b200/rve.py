@@ -536,6 +536,21 @@ class RVEBatch:
         )  # fmt: skip
         _native.check(code, "cib_rve_response")
 
+    def save_state(self, path) -> None:
+        """Write the committed state of every RVE (history, fluctuation, macro strain) to an
+        .npz file, for resuming long runs."""
+        np.savez(path, ep_n=self.ep_n.cpu().numpy(), q_n=self.q_n.cpu().numpy(), vpm_n=self.vpm_n.cpu().numpy(),
+                 w_n=self.w_n.cpu().numpy(), macro_n=self.macro_n.cpu().numpy(),
+                 elem_counts=self.elem_counts, precision=self.precision)  # fmt: skip
+
+    def load_state(self, path) -> None:
+        """Restore a committed state written by ``save_state`` for the same batch layout."""
+        data = np.load(path)
+        if not np.array_equal(data["elem_counts"], self.elem_counts) or int(data["precision"]) != self.precision:
+            raise ValueError("the saved state belongs to a batch of another layout or precision")
+        for name in ("ep_n", "q_n", "vpm_n", "w_n", "macro_n"):
+            getattr(self, name).copy_(torch.as_tensor(data[name], device=self.device))
+
     def commit(self) -> None:
         """Accept the trial state of every RVE as the committed state."""
         self.ep_n.copy_(self.ep)

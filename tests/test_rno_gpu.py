@@ -145,6 +145,22 @@ def test_training_divergence_guard_restores_finite_weights() -> None:
         assert torch.equal(L.w, w0) and bool(torch.isfinite(L.wb.float()).all())
 
 
+def test_checkpoint_resume_continues_training_exactly() -> None:
+    data = _material_point_dataset(P=256, T=50, seed=17)
+    scales = RNOScales.from_data(data.strain[:, 1:], data.rates(), data.stress[:, 1:])
+    cfg = RNOConfig(batch_paths=128, tbptt_steps=50, seed=3)
+    a = RNOSurrogate(cfg, scales)
+    a.fit(data, epochs=2)
+    ck = a.checkpoint()
+    b = RNOSurrogate(cfg, RNOScales(1.0, 1.0, 1.0))
+    b.load_checkpoint(ck)
+    ha, hb = a.fit(data, epochs=1), b.fit(data, epochs=1)
+    assert ha == hb
+    for La, Lb in zip(a.layers, b.layers):
+        assert torch.equal(La.w, Lb.w) and torch.equal(La.mw, Lb.mw)
+    assert int(a.step.item()) == int(b.step.item()) == 3 * 2
+
+
 def _material_point_dataset(P: int, T: int, seed: int, dt: float = 2.0e-6) -> RNODataset:
     """Macro stress paths of one viscoplastic mortar point (GPU return map) under random
     piecewise-linear strain paths (|strain| <= 2e-3) with a common time step."""

@@ -72,3 +72,24 @@ def test_auto_and_tuned_cluster_choice() -> None:
     out = R.tune_pcg_cluster(batch, UPDATE)
     assert set(out["ms"]) == {1, 2, 4, 8} and out["cluster"] in out["ms"]
     assert batch.cluster == out["cluster"]
+
+
+def test_saved_state_resumes_bitwise(tmp_path) -> None:
+    models = _models([8, 12], 64)
+    strains = np.random.default_rng(5).normal(0.0, 1.5e-3, size=(2, 6))
+    a = R.RVEBatch(models, precision=64)
+    a.macro.copy_(torch.as_tensor(strains, device=a.device))
+    a.dt.fill_(5.0e-6)
+    R.solve_batch_step(a, models[0].newton_settings, UPDATE, False)
+    a.commit()
+    a.save_state(tmp_path / "rve_state.npz")
+    b = R.RVEBatch(models, precision=64)
+    b.load_state(tmp_path / "rve_state.npz")
+    for batch in (a, b):
+        batch.macro.copy_(torch.as_tensor(2.0 * strains, device=batch.device))
+        batch.dt.fill_(5.0e-6)
+        R.solve_batch_step(batch, models[0].newton_settings, UPDATE, False)
+        batch.response(batch.batch_struct(UPDATE), batch.w, None, None)
+    assert torch.equal(a.sums, b.sums) and torch.equal(a.w, b.w)
+    with pytest.raises(ValueError, match="layout"):
+        R.RVEBatch(_models([8], 64), precision=64).load_state(tmp_path / "rve_state.npz")
