@@ -5,7 +5,9 @@
 // owns 128 paths for the whole window: the four weight matrices stay in shared memory in
 // the tcgen05 operand layout, the latent state stays in registers, and every time step
 // runs its four layers as back-to-back tcgen05.mma (M = 128, accumulator in TMEM) with the
-// bias/GELU epilogue writing the next layer's A operand straight into shared memory.
+// bias/GELU epilogue writing the next layer's A operand straight into shared memory.  The
+// epilogue is the step's critical path: 16 warps (four per TMEM lane quarter, each on a
+// quarter of the columns) share it.
 // The paths of a window are independent in time, so the recurrence needs no grid-wide
 // synchronisation.
 //
@@ -33,7 +35,10 @@ namespace {
 
 using namespace umma;
 
-constexpr int RW_THREADS = 256;
+constexpr int RW_THREADS = 512;
+constexpr int COL_GROUPS = RW_THREADS / 128;         // warps sharing one TMEM lane quarter
+constexpr int GROUP_COLS = 128 / COL_GROUPS;         // epilogue columns of each of them
+constexpr int GROUP_CHUNKS = GROUP_COLS / 16;        // 32x32b.x16 loads per layer and warp
 constexpr int HID = 128;
 constexpr int XIN = 32;
 constexpr int YOUT = 16;
@@ -104,7 +109,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
   extern __shared__ uint8_t smem_raw[];
   FwdSmem& S = *reinterpret_cast<FwdSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, half = warp >> 2;
+  const int quarter = warp & 3, group = warp >> 2;
   const int row = quarter * 32 + lane;
   const int B = w.B, T = w.T;
   const int p = blockIdx.x * TILE + row;
@@ -128,7 +133,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
   const bool has_skip = w.skip != nullptr;
 
   float z[6] = {0, 0, 0, 0, 0, 0};
-  if (half == 0 && valid)
+  if (group == 0 && valid)
 #pragma unroll
     for (int k = 0; k < 6; ++k) z[k] = w.z[(size_t)p * 6 + k];
   double sq = 0.0;
@@ -137,7 +142,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
   // inputs of the next step, loaded one step ahead so that their latency hides behind
   // the current step's layers
   float ne[6] = {0, 0, 0, 0, 0, 0}, nr[6] = {0, 0, 0, 0, 0, 0}, nt[6] = {0, 0, 0, 0, 0, 0}, nc = 0.0f;
-  if (half == 0 && valid) {
+  if (group == 0 && valid) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       ne[k] = w.strain[(size_t)p * 6 + k];
@@ -155,7 +160,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
       e[k] = ne[k];
       tg[k] = nt[k];
     }
-    if (half == 0) {
+    if (group == 0) {
       float xin[XIN];
 #pragma unroll
       for (int c2 = 0; c2 < XIN; ++c2) xin[c2] = 0.0f;
@@ -193,8 +198,8 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
       float* Zl = w.Z[l];
       __nv_bfloat16* Ht = static_cast<__nv_bfloat16*>(w.Ht[l]);
 #pragma unroll 1
-      for (int cb = 0; cb < 4; ++cb) {
-        const int c0 = 64 * half + 16 * cb;
+      for (int cb = 0; cb < GROUP_CHUNKS; ++cb) {
+        const int c0 = GROUP_COLS * group + 16 * cb;
         float v[16];
         tmem_ld16(lane_addr + (uint32_t)c0, v);
 #pragma unroll
@@ -217,7 +222,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
     // output layer and latent update
     ok = run_layer(&S.bar, tmem, S.h, S.w4, HID, YOUT, phase);
     if (!ok) break;
-    if (half == 0) {
+    if (group == 0) {
       float v[16];
       tmem_ld16(lane_addr, v);
       if (valid) {
@@ -279,7 +284,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
   extern __shared__ uint8_t smem_raw[];
   BwdSmem& S = *reinterpret_cast<BwdSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, half = warp >> 2;
+  const int quarter = warp & 3, group = warp >> 2;
   const int row = quarter * 32 + lane;
   const int B = w.B, T = w.T;
   const int p = blockIdx.x * TILE + row;
@@ -307,7 +312,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
   bool ok = true;
   // loss gradient and coefficient of the next (earlier) step, loaded one step ahead
   float ng[6] = {0, 0, 0, 0, 0, 0}, ncf = 0.0f;
-  if (half == 0 && valid) {
+  if (group == 0 && valid) {
     const size_t gl = (size_t)(T - 1) * B + p;
 #pragma unroll
     for (int k = 0; k < 6; ++k) ng[k] = w.gS[gl * 6 + k];
@@ -319,7 +324,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
 #pragma unroll
     for (int k = 0; k < 6; ++k) gs[k] = ng[k];
     const float cf = ncf;
-    if (half == 0) {
+    if (group == 0) {
       float dy[YOUT];
 #pragma unroll
       for (int c = 0; c < YOUT; ++c) dy[c] = 0.0f;
@@ -350,8 +355,8 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
       const float* Zl = w.Z[l];
       __nv_bfloat16* dZt = static_cast<__nv_bfloat16*>(w.dZt[l]);
 #pragma unroll 1
-      for (int cb = 0; cb < 4; ++cb) {
-        const int c0 = 64 * half + 16 * cb;
+      for (int cb = 0; cb < GROUP_CHUNKS; ++cb) {
+        const int c0 = GROUP_COLS * group + 16 * cb;
         float v[16];
         tmem_ld16(lane_addr + (uint32_t)c0, v);
         if (valid) {
@@ -378,7 +383,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
     // dX = dZ_1 W_1: the latent columns 12..17 feed dz
     ok = run_layer(&S.bar, tmem, S.d, S.w1t, HID, XIN, phase);
     if (!ok) break;
-    if (half == 0) {
+    if (group == 0) {
       float v0[16], v1[16];
       tmem_ld16(lane_addr, v0);
       tmem_ld16(lane_addr + 16u, v1);
