@@ -31,7 +31,7 @@ class TorchRNO(torch.nn.Module):
 def train_windows(strain, rate, stress, coef, windows: int, batch: int = 512, tbptt: int = 50, lr: float = 1e-3,
                   threads: int | None = None) -> dict:  # fmt: skip
     """Run ``windows`` TBPTT windows over normalised (P, T, 6) float32 inputs; returns the
-    seconds taken and the path-steps processed."""
+    seconds taken, the path-steps processed and the first and last window losses."""
     if threads:
         torch.set_num_threads(threads)
     torch.manual_seed(0)
@@ -40,6 +40,7 @@ def train_windows(strain, rate, stress, coef, windows: int, batch: int = 512, tb
     P, T = strain.shape[0], strain.shape[1]
     done, t0 = 0, time.perf_counter()
     w = 0
+    losses = []
     while w < windows:
         idx = torch.randperm(P)[:batch]
         z = torch.zeros(len(idx), 6)
@@ -51,9 +52,11 @@ def train_windows(strain, rate, stress, coef, windows: int, batch: int = 512, tb
             opt.zero_grad()
             (loss / tbptt).backward()
             opt.step()
+            losses.append(float(loss.detach()) / tbptt)
             z = z.detach()
             done += len(idx) * tbptt
             w += 1
             if w >= windows:
                 break
-    return {"seconds": time.perf_counter() - t0, "path_steps": done, "threads": torch.get_num_threads()}
+    return {"seconds": time.perf_counter() - t0, "path_steps": done, "threads": torch.get_num_threads(),
+            "loss_first": losses[0], "loss_last": losses[-1]}
