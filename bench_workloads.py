@@ -169,8 +169,9 @@ def run_rve_batch(args: argparse.Namespace) -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     setup = rve_batch_setup(256, 200)
+    forcing = os.environ.get("CIB_RVE_FORCING", "eisenstat_walker") or None
     with ClockSampler(local) as clocks:
-        out = rve_batch_workload(setup, args.warmup, args.steps)
+        out = rve_batch_workload(setup, args.warmup, args.steps, forcing=forcing)
     if rank != 0:
         return
     seconds = out["ms"] / 1e3
@@ -196,6 +197,7 @@ def run_rve_batch(args: argparse.Namespace) -> None:
                   "gauss_points": out["gauss_points"], "newton_max": out["newton_max"], "pcg_max": out["pcg_max"],
                   "pcg_total": out["pcg_total"], "plastic_fraction": out["plastic_fraction"],
                   "pcg_cluster": out["pcg_cluster"], "pcg_cluster_tuning_ms": (out["tuning"] or {}).get("ms"),
+                  "newton_forcing": out["forcing"],
                   "kernel_ms": out["kernel_ms"], "kernel_launches": out["kernel_launches"],
                   "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                "frac": None if achieved is None else achieved / peak, "traffic": None,

@@ -135,14 +135,16 @@ def rve_batch_setup(n_rve: int = 256, steps: int = 200, edges=EDGES, base_seed: 
     return RVEBatchSetup(models, np.asarray(times), np.asarray(strains))
 
 
-def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision: int = 32, tune: bool = True) -> dict:
+def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision: int = 32, tune: bool = True,
+                       forcing: str | None = "eisenstat_walker") -> dict:  # fmt: skip
     """Advance every RVE of the batch ``warmup`` path steps untimed, then ``timed`` steps
     timed; one step = one batched Newton solve (+ homogenisation and commit) per time index.
     Each step copies its macro strains and time steps from pinned host memory and reads the
     homogenised stresses back (the caller's view of the batched API).  With ``tune`` the PCG
     cluster size is measured (``tune_pcg_cluster``) on the first timed step's system before
-    the timed region."""
-    batch = RVEBatch(setup.models, precision=precision)
+    the timed region.  ``forcing`` selects the inexact-Newton PCG tolerance
+    (LinearSolverOptions.forcing)."""
+    batch = RVEBatch(setup.models, precision=precision, linear_solver=LinearSolverOptions(forcing=forcing))
     dev = batch.device
     strain_h = torch.as_tensor(setup.strains).pin_memory()
     dt_h = torch.as_tensor(np.diff(setup.times, axis=1)).pin_memory()
@@ -185,6 +187,7 @@ def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision:
             "stress_last": stress_h.numpy().copy(), "kernel_ms": kernel_ms, "kernel_launches": launches,
             "plastic_fraction": plastic, "h2d_bytes_per_step": int(batch.nrve * 7 * 8),
             "d2h_bytes_per_step": int(batch.nrve * 6 * 8), "pcg_cluster": int(batch.cluster), "tuning": tuning,
+            "forcing": forcing,
             "launches": launched,
             **counts}  # fmt: skip
 

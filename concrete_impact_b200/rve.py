@@ -193,11 +193,15 @@ class LinearSolverOptions:
     the reference solves directly).  ``relative_tolerance`` None picks 1e-11 for float64
     element kernels and 1e-6 for float32.  ``cluster`` is the number of CTAs (1, 2, 4, 8;
     one thread-block cluster) that share each linear system, or "auto" for a choice from
-    the batch's RVE sizes; ``tune_pcg_cluster`` measures the choice instead."""
+    the batch's RVE sizes; ``tune_pcg_cluster`` measures the choice instead.  ``forcing``
+    "eisenstat_walker" solves the Newton systems only as accurately as the Newton
+    iteration needs (the relative tolerance follows the residual's decrease, down to
+    ``relative_tolerance``); the Newton convergence tests are unchanged."""
 
     relative_tolerance: float | None = None
     max_iterations: int = 5000
     cluster: int | str = 1
+    forcing: str | None = None  # "eisenstat_walker": inexact Newton, see solve_batch_step
 
 
 @dataclass(frozen=True)
@@ -489,10 +493,12 @@ class RVEBatch:
             raise ValueError(f"PCG cluster {cluster} needs every RVE to have at least {cluster} element layers in z")
         return cluster
 
-    def pcg(self, b, rhs: torch.Tensor, x, r, p, Ap, nsys: int, sys_rve, sys_off, status, iters, rel, xnorm) -> None:
+    def pcg(self, b, rhs: torch.Tensor, x, r, p, Ap, nsys: int, sys_rve, sys_off, status, iters, rel, xnorm,
+            rtol: float | None = None) -> None:  # fmt: skip
         code = self.lib.cib_rve_pcg_cluster(
             ctypes.byref(b), nsys, sys_rve.data_ptr(), sys_off.data_ptr(), self.active.data_ptr(), rhs.data_ptr(),
-            self.dinv.data_ptr(), x.data_ptr(), r.data_ptr(), p.data_ptr(), Ap.data_ptr(), float(self.rtol),
+            self.dinv.data_ptr(), x.data_ptr(), r.data_ptr(), p.data_ptr(), Ap.data_ptr(),
+            float(self.rtol if rtol is None else rtol),
             int(self.linear.max_iterations), int(self.cluster), status.data_ptr(), iters.data_ptr(), rel.data_ptr(),
             xnorm.data_ptr(), _native.stream_ptr(),
         )  # fmt: skip
@@ -611,6 +617,11 @@ def solve_batch_step(
     pcg_total = np.zeros(R, dtype=np.int64)
     _set_active(batch, ~done)
     ns = newton
+    inexact = batch.linear.forcing == "eisenstat_walker"
+    if batch.linear.forcing not in (None, "eisenstat_walker"):
+        raise ValueError(f"unknown forcing {batch.linear.forcing!r}")
+    prev_rnorm = np.full(R, np.nan)
+    eta = 0.1
     for iteration in range(ns.max_iterations + 1):
         _timed(timers, "residual", lambda: batch.residual(b, batch.w, None, None))
         rn2, wn2, fail = (t.cpu().numpy() for t in (batch.rnorm2, batch.wnorm2, batch.fail))
@@ -631,9 +642,22 @@ def solve_batch_step(
             raise RVEEquilibriumError("maximum_iterations_exceeded", _failure_diag(batch, r, iteration, rnorm[r], tol[r],
                                                                                    last_inc[r], inc_tol[r]))  # fmt: skip
         _set_active(batch, live)
+        rtol = None
+        if inexact:
+            # Eisenstat-Walker choice 2 (gamma 0.9, alpha 2) over the live RVEs, with its
+            # safeguard, capped at 0.1 and floored at the solver's own tolerance
+            seen = live & np.isfinite(prev_rnorm) & (prev_rnorm > 0)
+            if seen.any():
+                ratio = float(np.max(rnorm[seen] / prev_rnorm[seen]))
+                new_eta = 0.9 * ratio**2
+                if 0.9 * eta**2 > 0.1:
+                    new_eta = max(new_eta, 0.9 * eta**2)
+                eta = min(new_eta, 0.1)
+            rtol = max(float(batch.rtol), eta)
+        prev_rnorm = np.where(live, rnorm, prev_rnorm)
         _timed(timers, "pcg", lambda: batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, R, batch.sys_rve,
                                                 batch.sys_off, batch.pcg_status, batch.pcg_iters, batch.pcg_rel,
-                                                batch.pcg_xnorm))  # fmt: skip
+                                                batch.pcg_xnorm, rtol))  # fmt: skip
         status, piters, xnorm = (t.cpu().numpy() for t in (batch.pcg_status, batch.pcg_iters, batch.pcg_xnorm))
         pcg_total[live] += piters[live]
         bad = live & ((status == 2) | ~np.isfinite(xnorm))

@@ -93,3 +93,25 @@ def test_saved_state_resumes_bitwise(tmp_path) -> None:
     assert torch.equal(a.sums, b.sums) and torch.equal(a.w, b.w)
     with pytest.raises(ValueError, match="layout"):
         R.RVEBatch(_models([8], 64), precision=64).load_state(tmp_path / "rve_state.npz")
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-6), (32, 1e-4)])
+def test_inexact_newton_forcing_reaches_the_same_state(precision: int, tol: float) -> None:
+    """Eisenstat-Walker PCG tolerances: the Newton convergence tests are unchanged, so the
+    homogenised stress agrees within the parity tolerances, with fewer PCG iterations."""
+    edges = [8, 12, 16, 8]
+    models = _models(edges, precision)
+    strains = np.random.default_rng(6).normal(0.0, 1.5e-3, size=(len(edges), 6))
+    out = {}
+    for forcing in (None, "eisenstat_walker"):
+        batch = R.RVEBatch(models, precision=precision, linear_solver=R.LinearSolverOptions(forcing=forcing))
+        batch.macro.copy_(torch.as_tensor(strains, device=batch.device))
+        batch.dt.fill_(5.0e-6)
+        res = R.solve_batch_step(batch, models[0].newton_settings, UPDATE, False)
+        batch.response(batch.batch_struct(UPDATE), batch.w, None, None)
+        vol = torch.as_tensor(batch.volumes, device=batch.device)[:, None]
+        out[forcing] = ((batch.sums[:, R.RS_SIGMA : R.RS_SIGMA + 6] / vol).cpu().numpy(), res)
+    ref, res_ref = out[None]
+    got, res = out["eisenstat_walker"]
+    assert np.all(np.abs(got - ref) <= tol * np.abs(ref).max(axis=1, keepdims=True))
+    assert res.pcg_iterations.sum() < res_ref.pcg_iterations.sum()
