@@ -194,6 +194,12 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_rno_gate_finish": (_I, [_I64, _P, _D, _P, _P, _P, _P, _P]),
     "cib_verlet_predict": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P]),
     "cib_verlet_correct": (_I, [_I64, _P, _D, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
+    "cib_hex8_mass_csr": (_I, [_I64, _P, _D, _I64, _P, _P, _P, _P, _P]),
+    "cib_newmark_kinematics": (_I, [_I64, _P, _P, _P, _D, _D, _P, _P, _P]),
+    "cib_newmark_residual": (_I, [_I64] + [_P] * 9),
+    "cib_newmark_effective_tangent": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P, _P, _P]),
+    "cib_csr_spmv": (_I, [_I64] + [_P] * 6),
+    "cib_csr_pcg": (_I, [_I64] + [_P] * 12 + [_D, ctypes.c_int32, ctypes.c_int32] + [_P] * 4),
     "cib_rve_residual": (_I, [_P] * 9),
     "cib_rve_gather": (_I, [_P] * 12),
     "cib_rve_pcg": (_I, [_P, ctypes.c_int32] + [_P] * 9 + [_D, ctypes.c_int32] + [_P] * 5),

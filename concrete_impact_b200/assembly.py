@@ -211,7 +211,7 @@ def assemble_hex8_material_response_cached(nodes, elements, material, committed_
         else:
             tangent = torch.sparse_csr_tensor(torch.as_tensor(cache.csr_indptr, device=dev),
                                               torch.as_tensor(cache.csr_indices, device=dev), values,
-                                              size=(n_dof, n_dof))  # fmt: skip
+                                              size=(n_dof, n_dof), check_invariants=False)  # fmt: skip
     else:
         tangent = csr_matrix((n_dof, n_dof)) if io.host else None
     return NonlinearSolidAssemblyResult(

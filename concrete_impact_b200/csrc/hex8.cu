@@ -4,6 +4,7 @@
 //   _build_hex8_quadrature_geometry   (src/fem/assembly/nonlinear_solid.py:391-425)
 //   _compute_hex8_strain_fields       (:428-454)
 //   _assemble_force_and_tangent       (:457-493)
+//   assemble_consistent_mass_matrix   (src/fem/assembly/elasticity.py:50-70, 109-140)
 // with the reference's conventions: lexicographic node signs (elements/lagrange.py:50-76),
 // 2x2x2 Gauss points in itertools.product order (quadrature/rules.py:24-33), DOF 3 n + c,
 // Voigt (xx, yy, zz, yz, xz, xy) with engineering shear (assembly/elasticity.py:160-183).
@@ -263,6 +264,37 @@ __global__ void __launch_bounds__(HEX_THREADS) hex8_stiffness_kernel(int64_t ne,
   for (int j = 0; j < 24; ++j) ke[(e * 24 + i) * 24 + j] = row[j];
 }
 
+// Trilinear shape value N_a at Gauss point q (same node signs and point order as ref_grad).
+__device__ __forceinline__ double shape_value(int q, int a) {
+  const double gp = 0.57735026918962576451;
+  const double xi = (q & 4) ? gp : -gp, eta = (q & 2) ? gp : -gp, zeta = (q & 1) ? gp : -gp;
+  const double sx = (a & 1) ? 1.0 : -1.0, sy = (a & 2) ? 1.0 : -1.0, sz = (a & 4) ? 1.0 : -1.0;
+  return 0.125 * (1.0 + sx * xi) * (1.0 + sy * eta) * (1.0 + sz * zeta);
+}
+
+// Element consistent mass me[e][i][j] = rho sum_q J w N_q(a_i) N_q(a_j) delta(d_i, d_j), in the
+// 24 x 24 layout of the element stiffness (src/fem/assembly/elasticity.py:109-140); one
+// thread per (e, i).
+__global__ void __launch_bounds__(HEX_THREADS) hex8_mass_kernel(int64_t ne, const double* __restrict__ jw, double density,
+                                                               double* __restrict__ me) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 24 * ne) return;
+  const int64_t e = t / 24;
+  const int i = (int)(t % 24);
+  const int ai = i / 3, di = i % 3;
+  double row[8];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) row[b] = 0.0;
+  for (int q = 0; q < 8; ++q) {
+    const double w = density * shape_value(q, ai) * jw[8 * e + q];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) row[b] += w * shape_value(q, b);
+  }
+  double* out = me + (e * 24 + i) * 24;
+#pragma unroll
+  for (int j = 0; j < 24; ++j) out[j] = (j % 3 == di) ? row[j / 3] : 0.0;
+}
+
 // CSR values: values[k] = sum over list[ptr[k] .. ptr[k+1]) of ke (fixed order).
 __global__ void __launch_bounds__(HEX_THREADS) csr_gather_kernel(int64_t nnz, const int64_t* __restrict__ ptr,
                                                                 const int64_t* __restrict__ list,
@@ -308,6 +340,15 @@ extern "C" int cib_hex8_internal_force(int64_t nelem, int64_t nnode, const doubl
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (nelem > 0) hex8_force_kernel<<<blocks_for(8 * nelem), HEX_THREADS, 0, st>>>(nelem, grads, jw, stress, fe);
   if (nnode > 0) hex8_node_gather_kernel<<<blocks_for(nnode), HEX_THREADS, 0, st>>>(nnode, node_ptr, node_list, fe, force);
+  return check_launch();
+}
+
+extern "C" int cib_hex8_mass_csr(int64_t nelem, const double* jw, double density, int64_t nnz, const int64_t* csr_ptr,
+                                 const int64_t* csr_list, double* me, double* values, void* stream) {
+  if (nelem < 0 || nnz < 0 || !jw || !csr_ptr || !csr_list || !me || !values || !(density > 0.0)) return CIB_EINVAL;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (nelem > 0) hex8_mass_kernel<<<blocks_for(24 * nelem), HEX_THREADS, 0, st>>>(nelem, jw, density, me);
+  if (nnz > 0) csr_gather_kernel<<<blocks_for(nnz), HEX_THREADS, 0, st>>>(nnz, csr_ptr, csr_list, me, values);
   return check_launch();
 }
 

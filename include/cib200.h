@@ -29,6 +29,10 @@
  *   cib_rve_*               solve_rve_microequilibrium and its assembly
  *                           (src/fem/rve/solver.py:62-227, 253-364, 438-461;
  *                           src/fem/assembly/nonlinear_solid.py:113-180, 428-493)
+ *   cib_hex8_mass_csr, cib_newmark_*, cib_csr_pcg
+ *                           assemble_consistent_mass_matrix and the implicit Newmark step
+ *                           (src/fem/assembly/elasticity.py:50-70, 109-140;
+ *                           src/fem/dynamics/material.py:300-701)
  */
 #ifndef CIB200_H
 #define CIB200_H
@@ -426,6 +430,51 @@ int cib_verlet_predict(int64_t n, const double* u, const double* v, const double
 int cib_verlet_correct(int64_t n, const double* f_unit, double load_scale, const double* f_int, const double* mass,
                        const uint8_t* fixed, double dt, const double* a, const double* v, double* a_next,
                        double* v_next, void* stream);
+
+/* --- Implicit macro dynamics (Newmark) -------------------------------------------------
+ * Device side of src/fem/dynamics/material.py:300-701 (solve_material_implicit_newmark,
+ * _solve_implicit_step, _evaluate_implicit_trial) on the CSR pattern of the Hex8 tangent
+ * (indptr/indices of n = 3N rows, int64).  free_mask[i] != 0 marks a free DOF; the
+ * homogeneous Dirichlet DOFs are the others. */
+
+/* Consistent mass (src/fem/assembly/elasticity.py:50-70, 109-140) in the CSR pattern and
+ * gather lists of cib_hex8_tangent_csr: element matrices into me (E*24*24, scratch), then the
+ * fixed-order gather into values (nnz). */
+int cib_hex8_mass_csr(int64_t nelem, const double* jw, double density, int64_t nnz, const int64_t* csr_ptr,
+                      const int64_t* csr_list, double* me, double* values, void* stream);
+
+/* a = (u - u_pred) / beta_dt2 and v = v_pred + gamma_dt * a (material.py:687-688). */
+int cib_newmark_kinematics(int64_t n, const double* u, const double* u_pred, const double* v_pred, double beta_dt2,
+                           double gamma_dt, double* a, double* v, void* stream);
+
+/* r = (M a + f_int) - f_ext on free rows, 0 on fixed rows (material.py:699). */
+int cib_newmark_residual(int64_t n, const int64_t* indptr, const int64_t* indices, const double* mass, const double* a,
+                         const double* f_int, const double* f_ext, const uint8_t* free_mask, double* r, void* stream);
+
+/* out = k_values + m_values / beta_dt2 (material.py:540; k_values may be NULL) and the Jacobi
+ * inverse diagonal dinv (1 / diag on free rows, 1 where diag <= 0, 0 on fixed rows). */
+int cib_newmark_effective_tangent(int64_t n, const int64_t* indptr, const int64_t* indices, const double* k_values,
+                                  const double* m_values, double beta_dt2, const uint8_t* free_mask, double* out,
+                                  double* dinv, void* stream);
+
+/* y = A x for a CSR matrix of n rows. */
+int cib_csr_spmv(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values, const double* x,
+                 double* y, void* stream);
+
+/* Jacobi-preconditioned CG for A x = b on the free rows (x = 0 on fixed rows), replacing the
+ * sparse direct solve of material.py:541-544 (src/fem/solvers/linear.py:15).  r, z, p, q are
+ * n-vectors of scratch, work CIB_CSR_PCG_WORK_DOUBLES doubles (device).  Stops when
+ * ||r|| <= rtol ||b|| or after maxit iterations; the host reads the device status every
+ * check_every iterations.  Host outputs: status 0 converged, 1 iteration limit, 2 breakdown
+ * (p.Ap <= 0 or a non-finite value); iterations; relative_residual ||r|| / ||b||.  The dot
+ * products are reduced in a fixed order: bitwise repeatable.  Returns CIB_ERANGE when n
+ * needs more than CIB_CSR_PCG_MAX_GRID blocks of partials. */
+#define CIB_CSR_PCG_MAX_GRID 1024
+#define CIB_CSR_PCG_WORK_DOUBLES (3 * CIB_CSR_PCG_MAX_GRID + 8)
+int cib_csr_pcg(int64_t n, const int64_t* indptr, const int64_t* indices, const double* values,
+                const uint8_t* free_mask, const double* dinv, const double* b, double* x, double* r, double* z,
+                double* p, double* q, double* work, double rtol, int32_t maxit, int32_t check_every, int32_t* status,
+                int32_t* iterations, double* relative_residual, void* stream);
 
 /* Error gate of the surrogate at n macro points (no reference counterpart; the reference's
  * deployment adapter, src/concrete_impact/nn/deployment.py:68-165, has no input gate).

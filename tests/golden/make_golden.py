@@ -251,26 +251,154 @@ def make_rve_cases():
     return cases
 
 
+def _newmark_bar(divisions, lengths, material):
+    """Duck-typed preprocess bundle of a structured bar: the fields the reference's
+    material-dynamics solver reads (mesh_info, shape_function_cache, material)."""
+    from types import SimpleNamespace
+
+    import fem.preprocess  # noqa: F401  (import order: fem.quadrature.cache imports fem.preprocess)
+    from fem.mesh.structured import build_structured_hex8_box
+    from fem.quadrature.cache import precompute_shape_functions
+
+    nodes, elements = build_structured_hex8_box(tuple(lengths), tuple(divisions))
+    nn = nodes.shape[0]
+    mesh_info = SimpleNamespace(nodes=nodes, elements=elements, element_type="hex8", dimension=3,
+                                dof_map=np.arange(3 * nn, dtype=np.int64).reshape(nn, 3))  # fmt: skip
+    cache = precompute_shape_functions(mesh_info, SimpleNamespace(quadrature={"order": 2}))
+    left = np.flatnonzero(np.isclose(nodes[:, 0], 0.0))
+    right = np.flatnonzero(np.isclose(nodes[:, 0], lengths[0]))
+    fixed = (3 * left[:, None] + np.arange(3)).ravel()
+    # consistent nodal force of a unit pressure on the x = L face (bilinear face, uniform)
+    unit = np.zeros(3 * nn)
+    ny, nz = divisions[1], divisions[2]
+    face = lengths[1] * lengths[2] / (ny * nz)
+    for k in range(nz):
+        for j in range(ny):
+            for dj, dk in ((0, 0), (1, 0), (0, 1), (1, 1)):
+                node = divisions[0] + (divisions[0] + 1) * ((j + dj) + (ny + 1) * (k + dk))
+                unit[3 * node] -= face / 4.0
+    bundle = SimpleNamespace(mesh_info=mesh_info, shape_function_cache=cache, material=material)
+    return bundle, nodes, elements, fixed, unit, right
+
+
+def _newmark_run(bundle, nodes, fixed, unit, amplitude, duration, dt, steps, adaptive, newton_args, armijo):
+    import math
+
+    from fem.dynamics.material import solve_material_implicit_newmark
+    from fem.materials.data import MaterialUpdateSettings
+    from fem.solvers.data import (AdaptiveTimeStepSettings, ArmijoSettings, DirichletDofSet, NonlinearNewtonSettings,
+                                  TimeIntegrationSettings)  # fmt: skip
+
+    def load(t):
+        return (amplitude * math.sin(math.pi * t / duration) if 0.0 <= t <= duration else 0.0) * unit
+
+    n_dof = 3 * nodes.shape[0]
+    sol = solve_material_implicit_newmark(
+        bundle, TimeIntegrationSettings("newmark", dt, steps, 0.25, 0.5, 1.0, AdaptiveTimeStepSettings(enabled=adaptive)),
+        np.zeros(n_dof), np.zeros(n_dof), DirichletDofSet(fixed, np.zeros(fixed.size)), load, "three_dimensional",
+        MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10),
+        NonlinearNewtonSettings(*newton_args, ArmijoSettings(enabled=armijo)))  # fmt: skip
+    arrays = {name: np.asarray(getattr(sol, name)) for name in (
+        "times", "displacement", "velocity", "acceleration", "stresses", "equivalent_plastic_strain",
+        "kinetic_energy", "free_energy", "dissipated_energy", "external_work", "energy_residual",
+        "newton_iterations", "armijo_backtracks", "accepted_time_steps", "rejected_step_counts")}  # fmt: skip
+    arrays["fixed_dofs"] = fixed
+    arrays["unit_force"] = unit
+    meta = {"amplitude": amplitude, "duration": duration, "time_step": dt, "num_steps": steps, "beta": 0.25,
+            "gamma": 0.5, "adaptive": adaptive, "newton": list(newton_args) + [armijo],
+            "update_settings": [50, 1.0e-10, 1.0e-12, 1.0e-10], "accepted_steps": int(arrays["times"].size - 1),
+            "rejected": int(arrays["rejected_step_counts"].sum()),
+            "rejected_reasons": [list(r) for r in sol.rejected_reasons]}  # fmt: skip
+    return arrays, meta
+
+
+def make_newmark_cases():
+    """Implicit Newmark material dynamics of the reference (solve_material_implicit_newmark)
+    on small pressure-pulse bars: J2 Perzyna at the macro points (fixed steps; adaptive
+    steps with Armijo and a two-iteration Newton budget that forces cutbacks), and FE2 with
+    a two-phase 4^3 RVE (RVEHomogenizedMaterial) at every macro point."""
+    from fem.materials.linear_elastic import LinearElasticMaterial
+    from fem.materials.phased import PhasedMaterialModel, RVEPhase
+    from fem.materials.plasticity import J2ViscoplasticMaterial
+    from fem.mesh.structured import build_structured_hex8_box
+    from fem.rve import StructuredHex8RVE, build_structured_hex8_periodic_constraint
+    from fem.rve.material import RVEHomogenizedMaterial
+    from fem.solvers.data import ArmijoSettings, NonlinearNewtonSettings
+
+    sys.path.insert(0, str(REPO))
+    from concrete_impact_b200.rve_builders import draw_spheres, sphere_phase_map
+
+    cases = {}
+    mortar = J2ViscoplasticMaterial("mortar", 2200.0, 25.0e9, 0.2, 20.0e6, 2.0e9, 1.0e-3, 20.0e6, 1.0)
+    bar = {"divisions": (6, 1, 1), "lengths": (0.06, 0.01, 0.01)}
+    bundle, nodes, elements, fixed, unit, _ = _newmark_bar(bar["divisions"], bar["lengths"], mortar)
+    runs = {
+        "newmark_j2_bar_fixed": dict(dt=2.0e-6, steps=20, adaptive=False, newton=(20, 1.0e-6, 1.0e-10, 1.0e-14, 1.0e-10),
+                                     armijo=False),
+        "newmark_j2_bar_adaptive": dict(dt=4.0e-6, steps=10, adaptive=True, newton=(2, 1.0e-6, 1.0e-10, 1.0e-14, 1.0e-10),
+                                        armijo=True),
+    }  # fmt: skip
+    for name, run in runs.items():
+        arrays, meta = _newmark_run(bundle, nodes, fixed, unit, 40.0e6, 20.0e-6, run["dt"], run["steps"],
+                                    run["adaptive"], run["newton"], run["armijo"])  # fmt: skip
+        meta.update(bar=bar, material=MATERIALS["mortar"])
+        cases[name] = (arrays, meta)
+    # FE2: the same bar geometry in 3 elements, a two-phase 4^3 RVE at each of the 24 points
+    aggregate = LinearElasticMaterial("aggregate", 2600.0, 50.0e9, 0.2)
+    div = (4, 4, 4)
+    rnodes, relements = build_structured_hex8_box((1.0, 1.0, 1.0), div)
+    phase = sphere_phase_map(div, draw_spheres(7))
+    frac = float(phase.mean())
+    density = 2200.0 * (1.0 - frac) + 2600.0 * frac
+    phased = PhasedMaterialModel("mortar__aggregate", (RVEPhase("matrix", mortar), RVEPhase("inclusion", aggregate)),
+                                 np.repeat(phase, 8), density)  # fmt: skip
+    rve_newton = NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=False))
+    model = StructuredHex8RVE(rnodes, relements, div, phased, build_structured_hex8_periodic_constraint(rnodes, div),
+                              rve_newton, element_phase_ids=phase, phase_names=("matrix", "inclusion"))  # fmt: skip
+    fe2_bar = {"divisions": (3, 1, 1), "lengths": (0.03, 0.01, 0.01)}
+    material = RVEHomogenizedMaterial(model, "two_phase_rve")
+    bundle, nodes, elements, fixed, unit, _ = _newmark_bar(fe2_bar["divisions"], fe2_bar["lengths"], material)
+    arrays, meta = _newmark_run(bundle, nodes, fixed, unit, 40.0e6, 10.0e-6, 2.0e-6, 8, False,
+                                (20, 1.0e-6, 1.0e-10, 1.0e-14, 1.0e-10), False)  # fmt: skip
+    arrays["element_phase"] = phase
+    meta.update(bar=fe2_bar, rve={"divisions": div, "seed": 7, "density": density,
+                                  "newton": [25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, False]})  # fmt: skip
+    cases["newmark_fe2_bar"] = (arrays, meta)
+    return cases
+
+
+GROUPS = ("j2", "rve", "newmark")
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--reference", default="/root/reference/src")
+    parser.add_argument("--only", choices=GROUPS, action="append",
+                        help="regenerate only these groups (default: all); the manifest keeps the other entries")
     args = parser.parse_args()
+    groups = set(args.only or GROUPS)
     _import_reference(args.reference)
     from fem.materials import data as data_mod
     from fem.materials import errors, plasticity
 
     cases = {}
-    cases.update(make_j2_cases(data_mod, plasticity))
-    cases.update(make_incremental_case(data_mod, plasticity))
-    cases.update(make_rve_cases())
-    manifest = {}
+    if "j2" in groups:
+        cases.update(make_j2_cases(data_mod, plasticity))
+        cases.update(make_incremental_case(data_mod, plasticity))
+    if "rve" in groups:
+        cases.update(make_rve_cases())
+    if "newmark" in groups:
+        cases.update(make_newmark_cases())
+    path = HERE / "manifest.json"
+    manifest = json.loads(path.read_text()) if path.exists() and args.only else {}
     for name, (arrays, meta) in cases.items():
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
         manifest[name] = json.loads(json.dumps(meta, default=lambda o: o.tolist() if hasattr(o, "tolist") else str(o)))
-    failures = make_failure_cases(data_mod, plasticity, errors)
-    (HERE / "j2_failures.json").write_text(json.dumps(failures, indent=1, sort_keys=True))
-    (HERE / "manifest.json").write_text(json.dumps(manifest, indent=1, sort_keys=True))
-    print("wrote", sorted(manifest), "and j2_failures.json")
+    if "j2" in groups:
+        failures = make_failure_cases(data_mod, plasticity, errors)
+        (HERE / "j2_failures.json").write_text(json.dumps(failures, indent=1, sort_keys=True))
+    path.write_text(json.dumps(manifest, indent=1, sort_keys=True))
+    print("wrote", sorted(cases))
 
 
 if __name__ == "__main__":
