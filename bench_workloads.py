@@ -13,6 +13,9 @@
 * fe2       -- the 64x16x16 impact bar with surrogate macro points behind the error gate;
   metric: macro steps/s, with all-direct FE^2 timed beside it and the surrogate's error
   against all-direct FP64 FE^2 on a 64x2x2 bar.
+* implicit_fe2 -- implicit Newmark FE^2 (solve_material_implicit_newmark) on a 16x4x4 bar
+  with an 8^3 concrete RVE (FP64) at each of the 2,048 macro points; metric: accepted macro
+  steps/s through the public call (host arrays in and out), RVE solves/s beside it.
 
 CPU baselines, each timed on the host on a bounded sample: the NumPy/SciPy oracle of the
 reference's RVE solve (direct sparse solves, the reference's algorithm) for rve_path,
@@ -378,15 +381,87 @@ def run_fe2(args: argparse.Namespace) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------
+# implicit_fe2
+
+IMPLICIT_FE2_POINTS = 2048
+IMPLICIT_FE2_EVALUATIONS = 3  # material evaluations per macro step assumed without a GPU run
+
+
+def _implicit_fe2_cpu(solves_per_step: float, solves: int = 3) -> dict:
+    """Implicit FE^2 on the host: the oracle's 8^3 RVE solve with its effective tangent (the
+    reference's algorithm, FP64 direct sparse solves) timed per solve, times the RVE solves
+    of one macro step, spread over all host cores without loss (which favours the CPU)."""
+    from concrete_impact_b200.benchmarks import concrete_rve
+
+    oracle = _oracle_for(concrete_rve(8, 0, 64), 1.0e-8)
+    state = oracle.initial_state()
+    t0 = time.perf_counter()
+    for k in range(1, solves + 1):
+        macro = np.array([-1.0e-3, 2.0e-4, 2.0e-4, 0.0, 0.0, 0.0]) * k / solves
+        state = oracle.solve(macro, 5.0e-6, state, True)["state"]
+    per_solve = (time.perf_counter() - t0) / solves
+    cores = os.cpu_count() or 1
+    return {"value": cores / (solves_per_step * per_solve), "unit": "macro steps/s", "cores": cores, "kind": "port",
+            "sample": f"oracle 8^3 RVE solves with effective tangent ({per_solve:.3f} s each, {solves} loading "
+                      f"steps) x {solves_per_step:.0f} RVE solves per macro step / {cores} cores"}  # fmt: skip
+
+
+def run_implicit_fe2(args: argparse.Namespace) -> None:
+    import torch
+
+    from bench import ClockSampler
+    from concrete_impact_b200.benchmarks import implicit_fe2_workload
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    with ClockSampler(local) as clocks:
+        out = implicit_fe2_workload(steps=args.steps, warmup=args.warmup)
+    if rank != 0:
+        return
+    seconds = out["ms"] / 1e3
+    value = out["steps"] / seconds
+    per_step = out["rve_solves"] / max(out["steps"], 1)
+    line = _line(args, "implicit FE2 accepted macro steps/s (16x4x4 Hex8 bar, 2,048 macro points, 8^3 concrete RVE "
+                       "per point, FP64, Newmark average acceleration)", value, "macro steps/s",
+                 "implicit_fe2: bar 0.16x0.04x0.04 m, x = 0 fixed, half-sine 40 MPa over 50 us, dt 5 us, "
+                 "macro Newton rel 1e-8, RVE Newton rel 1e-8",
+                 {"ms_per_step": out["ms"] / max(out["steps"], 1), "dtype": "f64",
+                  "rve_solves_per_s": out["rve_solves"] / seconds, "rve_solves_per_step": per_step,
+                  "micro_gp_per_rve": 8 * out["rve_elements"], "newton_iterations": out["newton_iterations"],
+                  "macro_pcg_iterations": out["macro_pcg_iterations"], "material_calls": out["material_calls"],
+                  "tip_displacement_m": out["tip_displacement"], "dissipated_energy_j": out["dissipated_energy"],
+                  "energy_residual_j": out["energy_residual"],
+                  "roofline": {"bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s", "frac": None,
+                               "traffic": None, "kernel": "rve_pcg (batched RVE Newton solves)",
+                               "note": "dominated by the batched RVE solves, whose PCG is latency-bound "
+                                       "(profiles/rve_pcg_cluster_batch256.md)"},
+                  "gpu_launches": out["launches"],
+                  "e2e": {"value": value, "unit": "macro steps/s",
+                          "h2d_bytes_per_step": out["h2d_bytes"] // max(out["steps"], 1),
+                          "d2h_bytes_per_step": out["d2h_record_bytes"] // max(out["steps"] + 1, 1),
+                          "path": "solve_material_implicit_newmark with host initial fields, host load vectors and "
+                                  "host histories; the whole call is the timed region (value and e2e are one measurement)"},
+                  "clocks": clocks.summary(),
+                  "cpu_baseline": None if args.no_cpu_baseline else _implicit_fe2_cpu(per_step)})  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args: argparse.Namespace) -> None:
     """``--impl reference``: the oracle alone on the workload's CPU sample (rank 0)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    if args.workload in ("rno_train", "fe2"):
-        c = _rno_train_cpu() if args.workload == "rno_train" else _fe2_cpu()
+    if args.workload in ("rno_train", "fe2", "implicit_fe2"):
+        if args.workload == "implicit_fe2":
+            c = _implicit_fe2_cpu(float(IMPLICIT_FE2_POINTS * IMPLICIT_FE2_EVALUATIONS))
+        else:
+            c = _rno_train_cpu() if args.workload == "rno_train" else _fe2_cpu()
         value, unit, sample = c["value"], c["unit"], c["sample"]
-        metric = ("surrogate training throughput (torch on the host)" if args.workload == "rno_train"
-                  else "direct FE2 macro steps/s (oracle RVE solves on the host)")  # fmt: skip
+        metric = {"rno_train": "surrogate training throughput (torch on the host)",
+                  "fe2": "direct FE2 macro steps/s (oracle RVE solves on the host)",
+                  "implicit_fe2": "implicit FE2 macro steps/s (oracle RVE solves with effective tangents on the host, "
+                                  f"{IMPLICIT_FE2_EVALUATIONS} material evaluations per step)"}[args.workload]  # fmt: skip
         line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32" if args.workload == "rno_train" else "f64", "data": "synthetic",
@@ -455,5 +530,7 @@ def run(args: argparse.Namespace) -> None:
         run_rno_train(args)
     elif args.workload == "fe2":
         run_fe2(args)
+    elif args.workload == "implicit_fe2":
+        run_implicit_fe2(args)
     else:
         raise SystemExit(f"unknown workload {args.workload}")

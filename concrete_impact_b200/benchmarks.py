@@ -17,6 +17,9 @@ rve_heterogeneous.py, dynamic_viscoplastic.py) for the concrete RVE of this pack
   (64 x 16 x 16 Hex8, 0.01 m elements, half-sine 50 MPa over 50 us, density 2400) with the
   surrogate at every macro point behind the error gate, checked against all-direct FE^2
   and timed against it.
+* ``implicit_fe2_workload`` -- implicit FE^2 through solve_material_implicit_newmark: a
+  16 x 4 x 4 Hex8 bar (0.01 m elements, 2,048 macro points) with an 8^3 concrete RVE (FP64)
+  at every point, average-acceleration Newmark at 5 us under a half-sine 40 MPa pulse.
 
 Each returns a dict of measured quantities; ``bench.py --workload`` prints them as its
 JSON line.  Timing uses CUDA events around whole steps on the current stream.
@@ -415,4 +418,82 @@ def fe2_speed(rno, envelope, rno_steps: int = 5000, rno_warmup: int = 5, direct_
                     "direct_steps_per_s": direct_steps / (sum(per_step) / 1e3)})  # fmt: skip
         del direct
         torch.cuda.empty_cache()
+    return out
+
+
+class _CountingMaterial:
+    """Delegates to a material and counts the macro points it solves."""
+
+    def __init__(self, inner) -> None:
+        self.inner = inner
+        self.points = 0
+        self.calls = 0
+
+    def __getattr__(self, name):
+        return getattr(self.inner, name)
+
+    def update(self, request, state, requirements=None):
+        self.points += int(request.strains.shape[0])
+        self.calls += 1
+        return self.inner.update(request, state, requirements) if requirements is not None else self.inner.update(
+            request, state)
+
+
+def implicit_fe2_workload(steps: int = 5, warmup: int = 3, divisions=(16, 4, 4), time_step: float = 5.0e-6,
+                          amplitude: float = 40.0e6, duration: float = 50.0e-6) -> dict:  # fmt: skip
+    """Accepted macro steps/s of implicit FE^2 (solve_material_implicit_newmark with an 8^3
+    concrete RVE at every macro point, FP64), through the public call with host arrays in
+    (initial fields, load vectors) and out (the recorded histories).  A ``warmup``-step run
+    from rest precedes the timed ``steps``-step run from rest; CUDA events bracket the call."""
+    from types import SimpleNamespace
+
+    from .dynamics import (DirichletDofSet, MacroOperators, TimeIntegrationSettings,
+                           solve_material_implicit_newmark)  # fmt: skip
+    from .fe2 import build_macro_bar, half_sine_pressure
+    from .rve import ArmijoSettings, NonlinearNewtonSettings
+    from .rve_material import RVEHomogenizedMaterial
+
+    model = concrete_rve(8, 0, 64)
+    material = _CountingMaterial(RVEHomogenizedMaterial(model, "concrete_rve_8"))
+    lengths = tuple(0.01 * d for d in divisions)
+    bar = build_macro_bar(divisions, lengths, material.density)
+    fixed = np.flatnonzero(bar.fixed.cpu().numpy())
+    unit = bar.unit_force.cpu().numpy()
+    mesh = SimpleNamespace(nodes=bar.nodes, elements=bar.elements, material=material)
+    h2d = [0]
+
+    def load(t: float) -> np.ndarray:
+        f = half_sine_pressure(t, amplitude, duration) * unit
+        h2d[0] += f.nbytes
+        return f
+
+    n = 3 * bar.nodes.shape[0]
+    newton = NonlinearNewtonSettings(20, 1.0e-3, 1.0e-8, 1.0e-14, 1.0e-8, ArmijoSettings(enabled=False))
+    dirichlet = DirichletDofSet(fixed, np.zeros(fixed.size))
+    ops = MacroOperators(bar.nodes, bar.elements, material.density, fixed, cache=bar.cache)
+
+    def call(k: int):
+        return solve_material_implicit_newmark(mesh, TimeIntegrationSettings("newmark", time_step, k, 0.25, 0.5, 1.0),
+                                               np.zeros(n), np.zeros(n), dirichlet, load, "three_dimensional",
+                                               UPDATE_SETTINGS, newton, operators=ops)  # fmt: skip
+
+    call(warmup)
+    material.points = material.calls = 0
+    h2d[0] = 0
+    calls0 = _native.LAUNCHED[0]
+    pcg0 = ops.linear_iterations
+    box: dict = {}
+    ms = _elapsed_ms(lambda: box.setdefault("sol", call(steps)))
+    sol = box["sol"]
+    accepted = int(sol.times.size - 1)
+    record_bytes = sum(getattr(sol, k).nbytes for k in ("displacement", "velocity", "acceleration", "internal_force",
+                                                         "external_force", "stresses", "equivalent_plastic_strain"))
+    out = {"ms": ms, "steps": accepted, "points": bar.points, "rve_elements": int(np.prod(model.divisions)),
+           "rve_solves": material.points, "material_calls": material.calls,
+           "newton_iterations": sol.newton_iterations[1:].tolist(), "macro_pcg_iterations": ops.linear_iterations - pcg0,
+           "launches": _native.LAUNCHED[0] - calls0, "h2d_bytes": h2d[0], "d2h_record_bytes": int(record_bytes),
+           "tip_displacement": float(sol.displacement[-1][3 * int(np.argmax(bar.nodes[:, 0]))]),
+           "dissipated_energy": float(sol.dissipated_energy[-1]), "external_work": float(sol.external_work[-1]),
+           "energy_residual": float(sol.energy_residual[-1]), "time_step": time_step}  # fmt: skip
+    material.inner.close()
     return out
