@@ -440,11 +440,13 @@ class _CountingMaterial:
 
 
 def implicit_fe2_workload(steps: int = 5, warmup: int = 3, divisions=(16, 4, 4), time_step: float = 5.0e-6,
-                          amplitude: float = 40.0e6, duration: float = 50.0e-6) -> dict:  # fmt: skip
+                          amplitude: float = 40.0e6, duration: float = 50.0e-6, forcing: str | None = None) -> dict:  # fmt: skip
     """Accepted macro steps/s of implicit FE^2 (solve_material_implicit_newmark with an 8^3
     concrete RVE at every macro point, FP64), through the public call with host arrays in
     (initial fields, load vectors) and out (the recorded histories).  A ``warmup``-step run
-    from rest precedes the timed ``steps``-step run from rest; CUDA events bracket the call."""
+    from rest precedes the timed ``steps``-step run from rest; CUDA events bracket the call.
+    ``forcing`` "eisenstat_walker" solves the RVE Newton systems inexactly (same RVE
+    convergence tests; see LinearSolverOptions)."""
     from types import SimpleNamespace
 
     from .dynamics import (DirichletDofSet, MacroOperators, TimeIntegrationSettings,
@@ -454,7 +456,8 @@ def implicit_fe2_workload(steps: int = 5, warmup: int = 3, divisions=(16, 4, 4),
     from .rve_material import RVEHomogenizedMaterial
 
     model = concrete_rve(8, 0, 64)
-    material = _CountingMaterial(RVEHomogenizedMaterial(model, "concrete_rve_8"))
+    linear = LinearSolverOptions(forcing=forcing) if forcing else None
+    material = _CountingMaterial(RVEHomogenizedMaterial(model, "concrete_rve_8", linear_solver=linear))
     lengths = tuple(0.01 * d for d in divisions)
     bar = build_macro_bar(divisions, lengths, material.density)
     fixed = np.flatnonzero(bar.fixed.cpu().numpy())
