@@ -109,7 +109,7 @@ def host_driver(monkeypatch):
     monkeypatch.setattr(D, "initialize_hex8_material_state",
                         lambda material, ne: MaterialState({"oracle": ctx["point"].initial_state(8 * ne)}))
 
-    def run(name: str, record_fields: bool = True):
+    def run(name: str, record_fields: bool = True, adaptive: bool | None = None):
         g, meta = load_case(name)
         nodes, elements = box_mesh(meta["bar"]["lengths"], meta["bar"]["divisions"])
         density = meta["material"]["density"]
@@ -122,7 +122,8 @@ def host_driver(monkeypatch):
             return (amp * math.sin(math.pi * t / dur) if 0.0 <= t <= dur else 0.0) * unit
 
         ts = D.TimeIntegrationSettings("newmark", meta["time_step"], meta["num_steps"], meta["beta"], meta["gamma"], 1.0,
-                                       D.AdaptiveTimeStepSettings(enabled=meta["adaptive"]))  # fmt: skip
+                                       D.AdaptiveTimeStepSettings(enabled=meta["adaptive"] if adaptive is None
+                                                                  else adaptive))  # fmt: skip
         newton = NonlinearNewtonSettings(*meta["newton"][:5], ArmijoSettings(enabled=meta["newton"][5]))
         n = ctx["ops"].n
         sol = D.solve_material_implicit_newmark(
@@ -173,3 +174,29 @@ def test_driver_rejects_inhomogeneous_dirichlet_and_other_kinematics(host_driver
         D.solve_material_implicit_newmark(mesh, ts, np.zeros(24), np.zeros(24), D.DirichletDofSet(np.array([0]),
                                           np.array([0.0])), lambda t: np.zeros(24), "plane_strain",
                                           MaterialUpdateSettings(50, 1e-10, 1e-12, 1e-10), newton)  # fmt: skip
+
+
+def test_unconverged_linear_solve_is_recoverable(host_driver, monkeypatch) -> None:
+    """A Newton system whose PCG solve stops at its iteration limit (status 1) fails the step
+    with the recoverable reason "linear_solver_not_converged": with fixed steps the error
+    propagates, with adaptive steps the step is retried at half the size."""
+    state = {"left": 1}
+    original = HostOperators.solve
+
+    def flaky(self, k_values, beta_dt2, rhs):
+        x, status, iterations, rel = original(self, k_values, beta_dt2, rhs)
+        if k_values is not None and state["left"] > 0:
+            state["left"] -= 1
+            return x, 1, 20000, 1e-3
+        return x, status, iterations, rel
+
+    monkeypatch.setattr(HostOperators, "solve", flaky)
+    with pytest.raises(D.RecoverableNonlinearStepError) as info:
+        host_driver("newmark_j2_bar_fixed")  # fixed steps: the failure propagates
+    assert info.value.reason == "linear_solver_not_converged"
+    assert info.value.diagnostics["linear_status"] == 1
+    state["left"] = 1
+    sol, g, _ = host_driver("newmark_j2_bar_fixed", adaptive=True)  # the first step is retried at half size
+    assert sol.rejected_reasons[1][0] == "linear_solver_not_converged"
+    assert sol.times[-1] == pytest.approx(g["times"][-1], rel=1e-12)
+    assert sol.accepted_time_steps[1] == pytest.approx(0.5 * g["accepted_time_steps"][1], rel=1e-12)
