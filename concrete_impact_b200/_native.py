@@ -195,6 +195,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_verlet_predict": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P]),
     "cib_verlet_correct": (_I, [_I64, _P, _D, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     "cib_hex8_mass_csr": (_I, [_I64, _P, _D, _I64, _P, _P, _P, _P, _P]),
+    "cib_csr_gather": (_I, [_I64] + [_P] * 5),
     "cib_newmark_kinematics": (_I, [_I64, _P, _P, _P, _D, _D, _P, _P, _P]),
     "cib_newmark_residual": (_I, [_I64] + [_P] * 9),
     "cib_newmark_effective_tangent": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P, _P, _P]),

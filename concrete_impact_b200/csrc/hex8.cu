@@ -343,6 +343,15 @@ extern "C" int cib_hex8_internal_force(int64_t nelem, int64_t nnode, const doubl
   return check_launch();
 }
 
+extern "C" int cib_csr_gather(int64_t nnz, const int64_t* ptr, const int64_t* list, const double* src, double* dst,
+                              void* stream) {
+  if (nnz < 0 || !ptr || !list || !src || !dst) return CIB_EINVAL;
+  if (nnz == 0) return CIB_OK;
+  csr_gather_kernel<<<blocks_for(nnz), HEX_THREADS, 0, reinterpret_cast<cudaStream_t>(stream)>>>(nnz, ptr, list, src,
+                                                                                                 dst);
+  return check_launch();
+}
+
 extern "C" int cib_hex8_mass_csr(int64_t nelem, const double* jw, double density, int64_t nnz, const int64_t* csr_ptr,
                                  const int64_t* csr_list, double* me, double* values, void* stream) {
   if (nelem < 0 || nnz < 0 || !jw || !csr_ptr || !csr_list || !me || !values || !(density > 0.0)) return CIB_EINVAL;

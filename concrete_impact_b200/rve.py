@@ -822,9 +822,30 @@ def _raise_material_failure(batch, fail, live, failure_context) -> None:
 # Single-RVE drop-in API.
 
 
+def is_structured_box(model: StructuredHex8RVE) -> bool:
+    """True when the model is a structured box of build_structured_hex8_box (the batched
+    box path); other meshes take the general-mesh path of ``rve_general``."""
+    try:
+        _check_structured(model)
+    except NotImplementedError:
+        return False
+    return True
+
+
 def build_rve_operator_cache(model: StructuredHex8RVE, precision: int = 64,
                              linear_solver: LinearSolverOptions | None = None) -> RVEOperatorCache:  # fmt: skip
-    """Geometry, quadrature weights, phase map and the device batch of one RVE."""
+    """Geometry, quadrature weights, phase map and the device batch of one RVE (for a
+    general mesh: its general-mesh operators, FP64)."""
+    if not is_structured_box(model):
+        from .rve_general import GeneralRVEOperators
+
+        if precision != 64:
+            raise NotImplementedError("General-mesh RVEs are solved in FP64 only.")
+        opts = linear_solver or LinearSolverOptions()
+        ops = GeneralRVEOperators(model, opts.relative_tolerance or 1.0e-11, opts.max_iterations)
+        phase_ids = (np.zeros(model.elements.shape[0], dtype=np.int64) if model.element_phase_ids is None
+                     else np.asarray(model.element_phase_ids, dtype=np.int64))  # fmt: skip
+        return RVEOperatorCache(ops.weights_host, ops.volume, np.repeat(phase_ids, 8), ops)
     hx, hy, hz = _check_structured(model)
     n_el = model.elements.shape[0]
     weights = np.full(8 * n_el, hx * hy * hz / 8.0)
@@ -911,6 +932,10 @@ def solve_rve_microequilibrium(
         raise ValueError("RVE time step must be positive.")
     if operator_cache is None or operator_cache.batch is None:
         operator_cache = build_rve_operator_cache(model)
+    if not isinstance(operator_cache.batch, RVEBatch):
+        from .rve_general import solve_general_rve_microequilibrium
+
+        return solve_general_rve_microequilibrium(model, request, committed_state, operator_cache.batch)
     batch: RVEBatch = operator_cache.batch
     io = _load_state(operator_cache, model, committed_state)
     batch.macro[0].copy_(torch.as_tensor(macro, device=batch.device))

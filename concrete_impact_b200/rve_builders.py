@@ -14,6 +14,13 @@
   Newton on the RVE's effective tangent around solve_rve_microequilibrium.
 * ``random_strain_path`` -- piecewise-linear 6-component macro strain path with a
   prescribed strain rate, for batched path generation.
+* ``build_cylindrical_ogrid_hex8`` / ``build_cylindrical_two_phase_rve`` -- the reference's
+  cylindrical two-phase RVE (src/fem/mesh/structured.py:83-154, 157-316;
+  src/fem/rve/builders.py:22-78): a centred z-cylinder inclusion meshed as a mapped square
+  core, a square annulus of matrix blended from the core boundary to the cell boundary,
+  extruded along z, with union-find periodic classes.  Same node, element and class
+  numbering as the reference (the RVE solve and its golden data index by them); solved by
+  the general-mesh RVE path of ``rve_general``.
 """
 
 from __future__ import annotations
@@ -30,6 +37,7 @@ from .rve import (
     RVEResponse,
     RVEState,
     StructuredHex8RVE,
+    build_periodic_constraint_from_classes,
     build_structured_hex8_box,
     build_structured_hex8_periodic_constraint,
 )
@@ -244,3 +252,175 @@ def describe(model: StructuredHex8RVE) -> dict[str, Any]:
     phase = model.element_phase_ids
     return {"divisions": model.divisions, "elements": int(model.elements.shape[0]),
             "inclusion_fraction": float(np.mean(phase)) if phase is not None else 0.0}  # fmt: skip
+
+
+# --------------------------------------------------------------------------------------
+# Cylindrical O-grid RVE.
+
+
+@dataclass(frozen=True)
+class CylindricalOGridHex8Mesh:
+    """Conforming Hex8 mesh of a periodic box with a centred z-cylinder inclusion."""
+
+    nodes: np.ndarray
+    elements: np.ndarray
+    element_phase_ids: np.ndarray
+    periodic_class_ids: np.ndarray
+    opposite_face_nodes: tuple
+    analytic_inclusion_area: float
+    discrete_inclusion_area: float
+
+
+def _ring_keys(c: int) -> list[tuple[int, int]]:
+    """Core-boundary grid keys (i, j), counterclockwise from (0, 0), each once."""
+    return ([(i, 0) for i in range(c)] + [(c, j) for j in range(c)] + [(i, c) for i in range(c, 0, -1)]
+            + [(0, j) for j in range(c, 0, -1)])  # fmt: skip
+
+
+def _ogrid_section(lx: float, ly: float, radius: float, c: int, m: int):
+    """Cross-section nodes (2D), quads, quad phases (1 core, 0 matrix) and the outer-ring
+    node -> grid key map.  Core node (i, j) is j (c + 1) + i at radius * (xi sqrt(1 - eta^2/2),
+    eta sqrt(1 - xi^2/2)); matrix ring r (1..m) blends each boundary key's core node towards
+    the cell boundary point (lx xi / 2, ly eta / 2) with weight r / m."""
+    t = np.linspace(-1.0, 1.0, c + 1)
+    xi, eta = np.meshgrid(t, t, indexing="xy")  # [j, i]
+    core = np.column_stack([(radius * xi * np.sqrt(1.0 - 0.5 * eta**2)).ravel(),
+                            (radius * eta * np.sqrt(1.0 - 0.5 * xi**2)).ravel()])  # fmt: skip
+    cid = lambda i, j: j * (c + 1) + i  # noqa: E731
+    quads = [[cid(i, j), cid(i + 1, j), cid(i, j + 1), cid(i + 1, j + 1)] for j in range(c) for i in range(c)]
+    phases = [1] * len(quads)
+    keys = _ring_keys(c)
+    ring_size = len(keys)
+    inner_ids = np.asarray([cid(i, j) for i, j in keys])
+    inner = core[inner_ids]
+    outer = np.column_stack([0.5 * lx * t[[i for i, _ in keys]], 0.5 * ly * t[[j for _, j in keys]]])
+    points = [core]
+    previous = inner_ids
+    count = core.shape[0]
+    for r in range(1, m + 1):
+        f = r / m
+        points.append((1.0 - f) * inner + f * outer)
+        current = count + np.arange(ring_size)
+        count += ring_size
+        nxt = (np.arange(ring_size) + 1) % ring_size
+        quads.extend(np.column_stack([previous[nxt], previous, current[nxt], current]).tolist())
+        phases.extend([0] * ring_size)
+        previous = current
+    outer_keys = {int(node): key for node, key in zip(previous, keys)}
+    return np.vstack(points), np.asarray(quads, dtype=np.int64), np.asarray(phases, dtype=np.int64), outer_keys
+
+
+def _ogrid_periodic_classes(cross_count: int, layers: int, outer_keys: dict):
+    """Union-find periodic classes (x, y pairs per layer in key order, then z pairs; the
+    second root is linked under the first) numbered by ascending root, and the opposite
+    face node lists."""
+    parent = np.arange((layers + 1) * cross_count, dtype=np.int64)
+
+    def root(a: int) -> int:
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = int(parent[a])
+        return a
+
+    def link(a: int, b: int) -> None:
+        ra, rb = root(a), root(b)
+        if ra != rb:
+            parent[rb] = ra
+
+    c = max(max(k) for k in outer_keys.values())
+    side = {name: {} for name in ("x-", "x+", "y-", "y+")}
+    for node, (i, j) in outer_keys.items():
+        if i == 0:
+            side["x-"][j] = node
+        if i == c:
+            side["x+"][j] = node
+        if j == 0:
+            side["y-"][i] = node
+        if j == c:
+            side["y+"][i] = node
+    faces = {name: [] for name in side}
+    for layer in range(layers + 1):
+        off = layer * cross_count
+        for axis in ("x", "y"):
+            minus, plus = side[axis + "-"], side[axis + "+"]
+            for key in sorted(minus):
+                link(off + minus[key], off + plus[key])
+                faces[axis + "-"].append(off + minus[key])
+                faces[axis + "+"].append(off + plus[key])
+    for node in range(cross_count):
+        link(node, layers * cross_count + node)
+    roots = np.asarray([root(a) for a in range(parent.size)], dtype=np.int64)
+    class_ids = np.unique(roots, return_inverse=True)[1].astype(np.int64)
+    bottom = np.arange(cross_count, dtype=np.int64)
+    face_nodes = ((np.asarray(faces["x-"], dtype=np.int64), np.asarray(faces["x+"], dtype=np.int64)),
+                  (np.asarray(faces["y-"], dtype=np.int64), np.asarray(faces["y+"], dtype=np.int64)),
+                  (bottom, layers * cross_count + bottom))  # fmt: skip
+    return class_ids, face_nodes
+
+
+def build_cylindrical_ogrid_hex8(lengths, inclusion_volume_fraction: float, circumferential_divisions: int,
+                                 matrix_radial_divisions: int, axial_divisions: int) -> CylindricalOGridHex8Mesh:  # fmt: skip
+    """Centred z-cylinder O-grid of a periodic box, extruded in axial_divisions layers.
+
+    Radius sqrt(f lx ly / pi); circumferential_divisions / 4 core divisions per side."""
+    if circumferential_divisions % 4 != 0:
+        raise ValueError("O-grid circumferential divisions must be divisible by four.")
+    if matrix_radial_divisions <= 0 or axial_divisions <= 0:
+        raise ValueError("O-grid radial and axial divisions must be positive.")
+    lx, ly, lz = (float(v) for v in lengths)
+    radius = float(np.sqrt(inclusion_volume_fraction * lx * ly / np.pi))
+    if radius >= 0.5 * min(lx, ly):
+        raise ValueError("Cylindrical inclusion intersects the periodic cell boundary.")
+    section, quads, phases, outer_keys = _ogrid_section(lx, ly, radius, circumferential_divisions // 4,
+                                                         matrix_radial_divisions)  # fmt: skip
+    nc = section.shape[0]
+    layers = axial_divisions
+    z = lz * np.arange(layers + 1) / layers
+    nodes = np.column_stack([np.tile(section, (layers + 1, 1)), np.repeat(z, nc)])
+    base = (np.arange(layers) * nc)[:, None, None]
+    elements = np.concatenate([base + quads[None, :, :], base + nc + quads[None, :, :]], axis=2).reshape(-1, 8)
+    element_phase = np.tile(phases, layers)
+    class_ids, face_nodes = _ogrid_periodic_classes(nc, layers, outer_keys)
+    q = section[quads[phases == 1]]  # (k, 4, 2): two triangles (0, 1, 2) and (1, 3, 2)
+    tri = lambda a, b, o: 0.5 * np.abs((a[:, 0] - o[:, 0]) * (b[:, 1] - o[:, 1]) - (a[:, 1] - o[:, 1]) * (b[:, 0] - o[:, 0]))  # noqa: E731,E501
+    area = float(np.sum(tri(q[:, 1], q[:, 2], q[:, 0]) + tri(q[:, 3], q[:, 2], q[:, 1])))
+    return CylindricalOGridHex8Mesh(nodes, elements.astype(np.int64), element_phase.astype(np.int64), class_ids,
+                                    face_nodes, float(np.pi * radius**2), area)  # fmt: skip
+
+
+def _element_volumes(nodes: np.ndarray, elements: np.ndarray) -> np.ndarray:
+    """Sum over the 2x2x2 Gauss points of det J per Hex8 element (host set-up)."""
+    g = 1.0 / np.sqrt(3.0)
+    pts = np.asarray([(a, b, c) for a in (-g, g) for b in (-g, g) for c in (-g, g)])
+    signs = np.asarray([[(-1.0, 1.0)[(a >> d) & 1] for d in range(3)] for a in range(8)])
+    f = 1.0 + pts[:, None, :] * signs[None, :, :]
+    dref = np.stack([0.125 * signs[None, :, 0] * f[:, :, 1] * f[:, :, 2], 0.125 * signs[None, :, 1] * f[:, :, 0] * f[:, :, 2],
+                     0.125 * signs[None, :, 2] * f[:, :, 0] * f[:, :, 1]], axis=2)  # fmt: skip
+    jac = np.einsum("eai,qaj->eqij", nodes[elements], dref)
+    return np.linalg.det(jac).sum(axis=1)
+
+
+def build_cylindrical_two_phase_rve(mesh: CylindricalOGridHex8Mesh, matrix_material, inclusion_material,
+                                    newton_settings: NonlinearNewtonSettings, hill_mandel_power_scale: float,
+                                    quadrature_order: int = 2) -> StructuredHex8RVE:  # fmt: skip
+    """Two-phase RVE on an O-grid: phase 0 matrix, phase 1 the cylindrical inclusion, the
+    effective density volume-weighted, periodic classes from the mesh topology."""
+    volumes = _element_volumes(mesh.nodes, mesh.elements)
+    vm = float(np.sum(volumes[mesh.element_phase_ids == 0]))
+    vi = float(np.sum(volumes[mesh.element_phase_ids == 1]))
+    density = (matrix_material.density * vm + inclusion_material.density * vi) / (vm + vi)
+    phased = PhasedMaterialModel(
+        name=f"{matrix_material.name}__{inclusion_material.name}",
+        phases=(RVEPhase("matrix", matrix_material), RVEPhase("inclusion", inclusion_material)),
+        point_phase_ids=np.repeat(mesh.element_phase_ids, 8),
+        effective_density=density,
+    )
+    constraint = build_periodic_constraint_from_classes(mesh.nodes, mesh.periodic_class_ids, (0, 0, 0),
+                                                        mesh.opposite_face_nodes)  # fmt: skip
+    return StructuredHex8RVE(
+        nodes=mesh.nodes, elements=mesh.elements, divisions=(0, 0, 0), material=phased, constraint=constraint,
+        newton_settings=newton_settings, element_phase_ids=mesh.element_phase_ids,
+        element_densities=np.where(mesh.element_phase_ids == 0, matrix_material.density, inclusion_material.density),
+        phase_names=("matrix", "inclusion"), quadrature_order=quadrature_order,
+        hill_mandel_power_scale=hill_mandel_power_scale,
+    )  # fmt: skip

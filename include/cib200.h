@@ -203,6 +203,12 @@ int cib_hex8_internal_force(int64_t nelem, int64_t nnode, const double* grads, c
 int cib_hex8_tangent_csr(int64_t nelem, const double* grads, const double* jw, const double* tangent, int64_t nnz,
                          const int64_t* csr_ptr, const int64_t* csr_list, double* ke, double* values, void* stream);
 
+/* dst[k] = sum of src[list[ptr[k] .. ptr[k+1])] in a fixed order, k < nnz: the values of a
+ * matrix whose entries are sums of another's, e.g. the reduced periodic tangent T^T K T of a
+ * general RVE mesh from the CSR tangent K (src/fem/rve/solver.py:143, 438-461). */
+int cib_csr_gather(int64_t nnz, const int64_t* ptr, const int64_t* list, const double* src, double* dst,
+                   void* stream);
+
 /* --- Periodic structured Hex8 RVE batch ------------------------------------------------
  * A batch holds R structured periodic RVEs (unit-cell boxes of nx*ny*nz Hex8 elements).
  * RVE r owns elements [elem_offset, elem_offset + nx*ny*nz); its periodic node (class)

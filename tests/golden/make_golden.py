@@ -367,7 +367,56 @@ def make_newmark_cases():
     return cases
 
 
-GROUPS = ("j2", "rve", "newmark")
+def make_ogrid_cases():
+    """The reference's cylindrical O-grid RVE (build_cylindrical_ogrid_hex8,
+    build_cylindrical_two_phase_rve): the mesh and its periodic topology, and three RVE
+    solves along a compression path with effective tangents (mortar J2 matrix, elastic
+    cylindrical inclusion)."""
+    from fem.materials.data import MaterialResponseRequirements, MaterialUpdateSettings
+    from fem.materials.linear_elastic import LinearElasticMaterial
+    from fem.materials.plasticity import J2ViscoplasticMaterial
+    from fem.mesh.structured import build_cylindrical_ogrid_hex8
+    from fem.rve import RVERequest, initialize_rve_state, solve_rve_microequilibrium
+    from fem.rve.builders import build_cylindrical_two_phase_rve
+    from fem.solvers.data import ArmijoSettings, NonlinearNewtonSettings
+
+    spec = {"lengths": (1.0, 1.0, 0.5), "inclusion_volume_fraction": 0.3, "circumferential_divisions": 8,
+            "matrix_radial_divisions": 2, "axial_divisions": 2}  # fmt: skip
+    mesh = build_cylindrical_ogrid_hex8(spec["lengths"], spec["inclusion_volume_fraction"],
+                                       spec["circumferential_divisions"], spec["matrix_radial_divisions"],
+                                       spec["axial_divisions"])  # fmt: skip
+    arrays = {"nodes": mesh.nodes, "elements": mesh.elements, "element_phase_ids": mesh.element_phase_ids,
+              "periodic_class_ids": mesh.periodic_class_ids}  # fmt: skip
+    for axis, (minus, plus) in zip("xyz", mesh.opposite_face_nodes):
+        arrays[f"face_{axis}_minus"] = np.asarray(minus)
+        arrays[f"face_{axis}_plus"] = np.asarray(plus)
+    mortar = J2ViscoplasticMaterial("mortar", 2200.0, 25.0e9, 0.2, 20.0e6, 2.0e9, 1.0e-3, 20.0e6, 1.0)
+    aggregate = LinearElasticMaterial("aggregate", 2600.0, 50.0e9, 0.2)
+    newton = NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=False))
+    model = build_cylindrical_two_phase_rve(mesh, mortar, aggregate, newton, 1.0)
+    update = MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10)
+    state = initialize_rve_state(model)
+    direction = np.asarray([-1.0, 0.22, 0.22, 0.05, -0.03, 0.08])
+    amplitudes = (0.6e-3, 1.4e-3, 2.2e-3)
+    scalars = []
+    for step, amp in enumerate(amplitudes):
+        macro = amp * direction
+        response = solve_rve_microequilibrium(
+            model, RVERequest(macro, 5.0e-6, update, MaterialResponseRequirements(tangent=True)), state)
+        a, sc = _rve_arrays(f"s{step}__", response, macro)
+        a[f"s{step}__displacement"] = response.displacement
+        arrays.update(a)
+        scalars.append(sc)
+        state = response.state
+    meta = {"mesh": spec, "analytic_inclusion_area": mesh.analytic_inclusion_area,
+            "discrete_inclusion_area": mesh.discrete_inclusion_area, "time_step": 5.0e-6, "steps": len(amplitudes),
+            "amplitudes": list(amplitudes), "direction": direction.tolist(), "scalars": scalars,
+            "newton": [25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, False], "hill_mandel_power_scale": 1.0,
+            "effective_density": float(model.material.density)}  # fmt: skip
+    return {"rve_ogrid_cylinder": (arrays, meta)}
+
+
+GROUPS = ("j2", "rve", "newmark", "ogrid")
 
 
 def main() -> None:
@@ -389,6 +438,8 @@ def main() -> None:
         cases.update(make_rve_cases())
     if "newmark" in groups:
         cases.update(make_newmark_cases())
+    if "ogrid" in groups:
+        cases.update(make_ogrid_cases())
     path = HERE / "manifest.json"
     manifest = json.loads(path.read_text()) if path.exists() and args.only else {}
     for name, (arrays, meta) in cases.items():
