@@ -42,7 +42,7 @@ WORKLOAD = "isolated batched return map, 16,777,216 GP SoA, FP64 state, tangent 
 FALLBACK_HBM_GBS = 6650.0
 # (timed steps, warm-up steps) per workload when not given on the command line
 WORKLOAD_DEFAULTS = {"return_map": (200, 5), "rve_path": (100, 3), "rve_batch": (5, 3), "rno_train": (300, 1),
-                     "fe2": (5000, 5), "implicit_fe2": (10, 3)}
+                     "fe2": (5000, 5), "implicit_fe2": (10, 3), "rve_ogrid": (20, 3)}
 
 
 def parse_args() -> argparse.Namespace:

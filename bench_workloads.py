@@ -13,6 +13,8 @@
 * fe2       -- the 64x16x16 impact bar with surrogate macro points behind the error gate;
   metric: macro steps/s, with all-direct FE^2 timed beside it and the surrogate's error
   against all-direct FP64 FE^2 on a 64x2x2 bar.
+* rve_ogrid -- the cylindrical O-grid two-phase RVE (2,560 general Hex8 elements) along a
+  20-step compression path; metric: accepted RVE steps/s through solve_prescribed_rve_path.
 * implicit_fe2 -- implicit Newmark FE^2 (solve_material_implicit_newmark) on a 16x4x4 bar
   with an 8^3 concrete RVE (FP64) at each of the 2,048 macro points; metric: accepted macro
   steps/s through the public call (host arrays in and out), RVE solves/s beside it.
@@ -382,6 +384,74 @@ def run_fe2(args: argparse.Namespace) -> None:
 
 
 # ---------------------------------------------------------------------------------------
+# rve_ogrid
+
+
+def _rve_ogrid_cpu(gpu_out: dict | None = None, sample_steps: int = 2) -> dict:
+    """The general-mesh RVE oracle (NumPy/SciPy, direct solves) on the first steps of the
+    same path; per-step time times the path's steps."""
+    from concrete_impact_b200.benchmarks import ogrid_path, ogrid_rve
+    from oracle import j2vp as oj
+    from oracle.rve import OraclePhase
+    from oracle.rve_general import general_rve_oracle
+
+    mesh, model = ogrid_rve()
+    newton = {"max_iterations": 25, "residual_absolute_tolerance": 1.0e-6, "residual_relative_tolerance": 1.0e-8,
+              "increment_absolute_tolerance": 1.0e-14, "increment_relative_tolerance": 1.0e-10, "armijo": None}  # fmt: skip
+    oracle = general_rve_oracle(mesh.nodes, mesh.elements, mesh.periodic_class_ids, int(mesh.opposite_face_nodes[0][0][0]),
+                                [OraclePhase("j2", oj.mortar_params()), OraclePhase("elastic", None, 50.0e9, 0.2)],
+                                mesh.element_phase_ids, newton)  # fmt: skip
+    steps = 20 if gpu_out is None else gpu_out["steps"]
+    times, strains = ogrid_path(steps)
+    state = oracle.initial_state()
+    diffs = []
+    t0 = time.perf_counter()
+    for k in range(1, sample_steps + 1):
+        out = oracle.solve(strains[k], float(times[k] - times[k - 1]), state, True)
+        state = out["state"]
+        if gpu_out is not None:
+            ref = np.asarray(gpu_out["macro_stress"][k - 1])
+            diffs.append(float(np.abs(out["macro_stress"] - ref).max() / np.abs(ref).max()))
+    per_step = (time.perf_counter() - t0) / sample_steps
+    line = {"value": 1.0 / per_step, "unit": "RVE steps/s", "cores": 1, "kind": "port",
+            "sample": f"general-mesh RVE oracle on the first {sample_steps} path steps, {per_step:.3f} s per step"}  # fmt: skip
+    if diffs:
+        line["max_rel_stress_diff_vs_gpu"] = max(diffs)
+    return line
+
+
+def run_rve_ogrid(args: argparse.Namespace) -> None:
+    import torch
+
+    from bench import ClockSampler
+    from concrete_impact_b200.benchmarks import ogrid_rve_path_workload
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    with ClockSampler(local) as clocks:
+        out = ogrid_rve_path_workload(steps=args.steps, warmup=args.warmup)
+    if rank != 0:
+        return
+    seconds = out["ms"] / 1e3
+    value = out["steps"] / seconds
+    line = _line(args, "accepted RVE steps/s (cylindrical O-grid two-phase RVE, general Hex8 mesh, FP64)", value,
+                 "RVE steps/s", f"rve_ogrid: 32x8x8 O-grid, {out['elements']} elements, {out['dofs']} DOF, 30 % "
+                                "aggregate cylinder, proportional compression to 2.5e-3 in 20 steps, dt 5 us",
+                 {"ms_per_step": out["ms"] / max(out["steps"], 1), "dtype": "f64",
+                  "gp_evaluations_per_s": out["evaluations"] / seconds, "newton_iterations": out["newton_iterations"],
+                  "final_macro_stress_pa": out["macro_stress"][-1],
+                  "roofline": {"bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s", "frac": None,
+                               "traffic": None, "note": "one small RVE: launch- and latency-bound CSR kernels"},
+                  "gpu_launches": out["launches"],
+                  "e2e": {"value": value, "unit": "RVE steps/s", "h2d_bytes_per_step": 6 * 8,
+                          "d2h_bytes_per_step": (6 + 36) * 8,
+                          "path": "solve_prescribed_rve_path with host arrays in and out (value and e2e are one measurement)"},
+                  "clocks": clocks.summary(), "cpu_baseline": None if args.no_cpu_baseline else _rve_ogrid_cpu(out)})  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
 # implicit_fe2
 
 IMPLICIT_FE2_POINTS = 2048
@@ -453,16 +523,19 @@ def run_reference(args: argparse.Namespace) -> None:
     """``--impl reference``: the oracle alone on the workload's CPU sample (rank 0)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    if args.workload in ("rno_train", "fe2", "implicit_fe2"):
+    if args.workload in ("rno_train", "fe2", "implicit_fe2", "rve_ogrid"):
         if args.workload == "implicit_fe2":
             c = _implicit_fe2_cpu(float(IMPLICIT_FE2_POINTS * IMPLICIT_FE2_EVALUATIONS))
+        elif args.workload == "rve_ogrid":
+            c = _rve_ogrid_cpu()
         else:
             c = _rno_train_cpu() if args.workload == "rno_train" else _fe2_cpu()
         value, unit, sample = c["value"], c["unit"], c["sample"]
         metric = {"rno_train": "surrogate training throughput (torch on the host)",
                   "fe2": "direct FE2 macro steps/s (oracle RVE solves on the host)",
                   "implicit_fe2": "implicit FE2 macro steps/s (oracle RVE solves with effective tangents on the host, "
-                                  f"{IMPLICIT_FE2_EVALUATIONS} material evaluations per step)"}[args.workload]  # fmt: skip
+                                  f"{IMPLICIT_FE2_EVALUATIONS} material evaluations per step)",
+                  "rve_ogrid": "accepted RVE steps/s (general-mesh RVE oracle, cylindrical O-grid)"}[args.workload]  # fmt: skip
         line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32" if args.workload == "rno_train" else "f64", "data": "synthetic",
@@ -533,5 +606,7 @@ def run(args: argparse.Namespace) -> None:
         run_fe2(args)
     elif args.workload == "implicit_fe2":
         run_implicit_fe2(args)
+    elif args.workload == "rve_ogrid":
+        run_rve_ogrid(args)
     else:
         raise SystemExit(f"unknown workload {args.workload}")

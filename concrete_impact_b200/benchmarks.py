@@ -17,6 +17,9 @@ rve_heterogeneous.py, dynamic_viscoplastic.py) for the concrete RVE of this pack
   (64 x 16 x 16 Hex8, 0.01 m elements, half-sine 50 MPa over 50 us, density 2400) with the
   surrogate at every macro point behind the error gate, checked against all-direct FE^2
   and timed against it.
+* ``ogrid_rve_path_workload`` -- the cylindrical O-grid two-phase RVE (32 circumferential,
+  8 radial, 8 axial divisions: 2,560 elements, 30 % inclusion) along a 20-step compression
+  path through solve_prescribed_rve_path (general-mesh device path, FP64).
 * ``implicit_fe2_workload`` -- implicit FE^2 through solve_material_implicit_newmark: a
   16 x 4 x 4 Hex8 bar (0.01 m elements, 2,048 macro points) with an 8^3 concrete RVE (FP64)
   at every point, average-acceleration Newmark at 5 us under a half-sine 40 MPa pulse.
@@ -500,3 +503,43 @@ def implicit_fe2_workload(steps: int = 5, warmup: int = 3, divisions=(16, 4, 4),
            "energy_residual": float(sol.energy_residual[-1]), "time_step": time_step}  # fmt: skip
     material.inner.close()
     return out
+
+
+OGRID_DIRECTION = np.asarray([-1.0, 0.22, 0.22, 0.05, -0.03, 0.08])
+
+
+def ogrid_rve(circumferential: int = 32, radial: int = 8, axial: int = 8):
+    """Cylindrical O-grid concrete RVE: mortar matrix (J2 Perzyna), elastic aggregate
+    cylinder at 30 % of the unit cell, Newton relative tolerance 1e-8."""
+    from .rve_builders import build_cylindrical_ogrid_hex8, build_cylindrical_two_phase_rve
+
+    mortar, aggregate = config0_materials()
+    mesh = build_cylindrical_ogrid_hex8((1.0, 1.0, 1.0), 0.3, circumferential, radial, axial)
+    return mesh, build_cylindrical_two_phase_rve(mesh, mortar, aggregate, default_newton(), 1.0)
+
+
+def ogrid_path(steps: int, final_amplitude: float = 2.5e-3, time_step: float = 5.0e-6):
+    """Times and macro strains of a proportional compression path from rest."""
+    times = time_step * np.arange(steps + 1)
+    strains = np.outer(np.linspace(0.0, final_amplitude, steps + 1), OGRID_DIRECTION)
+    return times, strains
+
+
+def ogrid_rve_path_workload(steps: int = 20, warmup: int = 3) -> dict:
+    """Accepted RVE steps/s of the O-grid RVE along ``ogrid_path(steps)`` through
+    solve_prescribed_rve_path; a ``warmup``-step path first, CUDA events around the call."""
+    from .rve import solve_prescribed_rve_path
+
+    mesh, model = ogrid_rve()
+    solve_prescribed_rve_path(model, *ogrid_path(warmup), UPDATE_SETTINGS)
+    times, strains = ogrid_path(steps)
+    calls0 = _native.LAUNCHED[0]
+    box: dict = {}
+    ms = _elapsed_ms(lambda: box.setdefault("r", solve_prescribed_rve_path(model, times, strains, UPDATE_SETTINGS)))
+    result = box["r"]
+    newton = [int(r.diagnostics["newton_iterations"]) for r in result.responses]
+    return {"ms": ms, "steps": len(result.responses), "elements": int(model.elements.shape[0]),
+            "dofs": 3 * int(model.nodes.shape[0]), "newton_iterations": newton,
+            "evaluations": 8 * int(model.elements.shape[0]) * (sum(newton) + len(newton)),
+            "launches": _native.LAUNCHED[0] - calls0, "macro_stress": [np.asarray(r.macro_stress).tolist() for r in result.responses],
+            "times": times, "strains": strains, "mesh": mesh}  # fmt: skip
