@@ -10,12 +10,12 @@ tangent=True).  Headline precision is float64 (the reference's); the float32 var
 the method is reported alongside.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload return_map|rve_path|rve_batch|rno_train|fe2]
+                    [--workload return_map|rve_path|rve_batch|rno_train|fe2|implicit_fe2|rve_ogrid]
 
 Under torchrun each rank updates its own batch of the same size (independent points:
 weak scaling, no collective on the data path); rank 0 prints the line.  The other
-workloads (the RVE path, the 256-RVE batch, surrogate training and FE^2) are in
-bench_workloads.py.
+workloads (the RVE path, the 256-RVE batch, surrogate training, explicit and implicit
+FE^2, the cylindrical O-grid RVE path) are in bench_workloads.py.
 """
 
 from __future__ import annotations

@@ -1,4 +1,5 @@
-"""The workloads of ``bench.py --workload rve_path|rve_batch|rno_train|fe2`` (one JSON line on rank 0).
+"""The workloads of ``bench.py --workload rve_path|rve_batch|rno_train|fe2|implicit_fe2|rve_ogrid``
+(one JSON line on rank 0).
 
 * rve_path  -- one 8^3 two-phase concrete RVE, mixed-control uniaxial compression to
   -0.5 % in 100 steps at 10 /s (free components at zero macro stress), FP64.  Metric:
@@ -21,8 +22,8 @@
 
 CPU baselines, each timed on the host on a bounded sample: the NumPy/SciPy oracle of the
 reference's RVE solve (direct sparse solves, the reference's algorithm) for rve_path,
-rve_batch and fe2, and the torch training loop on the host (oracle/rno_torch.py) for
-rno_train.
+rve_batch, fe2 and implicit_fe2, its general-mesh form for rve_ogrid, and the torch
+training loop on the host (oracle/rno_torch.py) for rno_train.
 Multi-GPU runs are replicas: every rank runs the same workload, rank 0 prints.
 """
 
