@@ -159,6 +159,20 @@ class RNOWindowC(ctypes.Structure):
     ]
 
 
+class EnergyRNOC(ctypes.Structure):
+    """``cib_energy_rno``."""
+
+    _fields_ = [
+        ("hidden", ctypes.c_int32),
+        ("layers", ctypes.c_int32),
+        ("latent", ctypes.c_int32),
+        ("integrator", ctypes.c_int32),
+        ("reference_time_scale", ctypes.c_double),
+        ("params", ctypes.c_void_p),
+        ("strain_scale", ctypes.c_void_p),
+    ]
+
+
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
 _D = ctypes.c_double
@@ -196,6 +210,9 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_verlet_correct": (_I, [_I64, _P, _D, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     "cib_hex8_mass_csr": (_I, [_I64, _P, _D, _I64, _P, _P, _P, _P, _P]),
     "cib_csr_gather": (_I, [_I64] + [_P] * 5),
+    "cib_energy_rno_param_count": (_I64, [ctypes.c_int32] * 3),
+    "cib_energy_rno_anchors": (_I, [_P, _P, _P]),
+    "cib_energy_rno_update": (_I, [_P, _I64] + [_P] * 10),
     "cib_newmark_kinematics": (_I, [_I64, _P, _P, _P, _D, _D, _P, _P, _P]),
     "cib_newmark_residual": (_I, [_I64] + [_P] * 9),
     "cib_newmark_effective_tangent": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P, _P, _P]),

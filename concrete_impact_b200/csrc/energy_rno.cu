@@ -1,0 +1,396 @@
+// Energy-based RVE-RNO update on the GPU (FP32), sm_100a.
+//
+// Restates the reference's EnergyDissipationRVERNO._constitutive_tensors
+// (src/concrete_impact/nn/models/rve_rno.py:334-418; direct_rate evolution, both
+// integrators), ScalarMLP.value_and_input_gradient (:110-129), the SiLU MultilayerPerceptron
+// (:63-93) and prepare_energy_anchors (:227-247).  Per point and step: the equilibrium
+// potential and its strain gradient, the non-equilibrium potential and its gradient at the
+// previous state, the state-evolution network there, the forward-Euler latent candidate,
+// and the non-equilibrium potential and gradient at the candidate -- four network passes and
+// three hand-written input-gradient passes of 6/12 -> hidden^layers -> 1 (or 6) networks.
+//
+// One CTA of 128 threads per tile of 32 points.  Forward layers: thread j owns hidden unit j
+// and keeps the 32 points' accumulators in registers; the layer's input rows sit in shared
+// memory (broadcast reads) and the transposed weights are read along j (coalesced).
+// Input-gradient layers: thread k owns input k and reads the weights along k (coalesced).
+// Pre-activations of every layer stay in shared memory for the backward pass; shared rows
+// are padded to hidden + 1 floats so that per-point column reads hit distinct banks.
+// Everything is FP32 like the reference model (its dtype float32); no waits besides
+// __syncthreads.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "cib_common.cuh"
+
+namespace cib {
+namespace {
+
+constexpr int ER_TILE = 32;
+constexpr int ER_THREADS = 128;
+constexpr int ER_XLD = 16;  // input rows: 6 + latent <= 14, padded
+
+// Parameter layout of one network (floats), for each hidden layer l: W [hidden][in_l],
+// Wt [in_l][hidden], b [hidden]; then Wo [out][hidden], bo [out].
+__host__ __device__ inline int64_t net_size(int in, int out, int hidden, int layers) {
+  int64_t s = 0;
+  for (int l = 0; l < layers; ++l) {
+    const int in_l = l == 0 ? in : hidden;
+    s += 2LL * hidden * in_l + hidden;
+  }
+  return s + (int64_t)out * hidden + out;
+}
+
+struct NetView {
+  const float* base;
+  int in, out;
+};
+
+__device__ __forceinline__ void layer_ptrs(const NetView& n, int hidden, int l, const float** W, const float** Wt,
+                                           const float** b) {
+  const float* p = n.base;
+  for (int i = 0; i < l; ++i) {
+    const int in_i = i == 0 ? n.in : hidden;
+    p += 2LL * hidden * in_i + hidden;
+  }
+  const int in_l = l == 0 ? n.in : hidden;
+  *W = p;
+  *Wt = p + (int64_t)hidden * in_l;
+  *b = p + 2LL * hidden * in_l;
+}
+
+__device__ __forceinline__ const float* output_ptr(const NetView& n, int hidden, int layers) {
+  const float* p = n.base;
+  for (int i = 0; i < layers; ++i) {
+    const int in_i = i == 0 ? n.in : hidden;
+    p += 2LL * hidden * in_i + hidden;
+  }
+  return p;  // Wo [out][hidden], then bo [out]
+}
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
+
+__device__ __forceinline__ float silu_prime(float z) {
+  const float s = 1.0f / (1.0f + expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+struct Smem {
+  float* x;     // [TILE][XLD] network input
+  float* z;     // [layers][TILE][LD] pre-activations
+  float* h0;    // [TILE][LD]
+  float* h1;    // [TILE][LD]
+  float* gin;   // [TILE][XLD] input gradient
+  int ld;
+};
+
+// Forward pass of the hidden layers; returns the buffer holding the last activation.
+__device__ float* forward_hidden(const NetView& n, int hidden, int layers, const Smem& s) {
+  const int j = threadIdx.x;
+  const float* hin = s.x;
+  int ldin = ER_XLD;
+  float* hout = s.h0;
+  for (int l = 0; l < layers; ++l) {
+    const float *W, *Wt, *b;
+    layer_ptrs(n, hidden, l, &W, &Wt, &b);
+    const int in_l = l == 0 ? n.in : hidden;
+    float* zl = s.z + (int64_t)l * ER_TILE * s.ld;
+    if (j < hidden) {
+      float acc[ER_TILE];
+      const float bj = b[j];
+#pragma unroll
+      for (int p = 0; p < ER_TILE; ++p) acc[p] = bj;
+      for (int k = 0; k < in_l; ++k) {
+        const float w = Wt[(int64_t)k * hidden + j];
+#pragma unroll
+        for (int p = 0; p < ER_TILE; ++p) acc[p] = fmaf(w, hin[p * ldin + k], acc[p]);
+      }
+#pragma unroll
+      for (int p = 0; p < ER_TILE; ++p) {
+        zl[p * s.ld + j] = acc[p];
+        hout[p * s.ld + j] = silu(acc[p]);
+      }
+    }
+    __syncthreads();
+    hin = hout;
+    ldin = s.ld;
+    hout = (hout == s.h0) ? s.h1 : s.h0;
+  }
+  return const_cast<float*>(hin);
+}
+
+// Scalar potential value per point (threads p < TILE) into value[p].
+__device__ void scalar_output(const NetView& n, int hidden, int layers, const float* h, int ld, float* value) {
+  const float* wo = output_ptr(n, hidden, layers);
+  const int p = threadIdx.x;
+  if (p < ER_TILE) {
+    float v = 0.0f;
+    for (int j = 0; j < hidden; ++j) v = fmaf(wo[j], h[p * ld + j], v);
+    value[p] = v;
+  }
+  __syncthreads();
+}
+
+// Input gradient of a scalar network into s.gin[p][0..in) (pre-activations in s.z).
+__device__ void input_gradient(const NetView& n, int hidden, int layers, const Smem& s) {
+  const float* wo = output_ptr(n, hidden, layers);
+  const int t = threadIdx.x;
+  float* g = s.h0;  // gradient wrt the activation of layer l (rows TILE x ld)
+  float* d = s.h1;  // gradient wrt the pre-activation of layer l
+  for (int l = layers - 1; l >= 0; --l) {
+    const float* zl = s.z + (int64_t)l * ER_TILE * s.ld;
+    if (t < hidden) {
+#pragma unroll 4
+      for (int p = 0; p < ER_TILE; ++p) {
+        const float gv = (l == layers - 1) ? wo[t] : g[p * s.ld + t];
+        d[p * s.ld + t] = gv * silu_prime(zl[p * s.ld + t]);
+      }
+    }
+    __syncthreads();
+    const float *W, *Wt, *b;
+    layer_ptrs(n, hidden, l, &W, &Wt, &b);
+    const int in_l = l == 0 ? n.in : hidden;
+    float* dst = l == 0 ? s.gin : g;
+    const int lddst = l == 0 ? ER_XLD : s.ld;
+    if (t < in_l) {
+      float acc[ER_TILE];
+#pragma unroll
+      for (int p = 0; p < ER_TILE; ++p) acc[p] = 0.0f;
+      for (int jj = 0; jj < hidden; ++jj) {
+        const float w = W[(int64_t)jj * in_l + t];
+#pragma unroll
+        for (int p = 0; p < ER_TILE; ++p) acc[p] = fmaf(d[p * s.ld + jj], w, acc[p]);
+      }
+#pragma unroll
+      for (int p = 0; p < ER_TILE; ++p) dst[p * lddst + t] = acc[p];
+    }
+    __syncthreads();
+  }
+}
+
+struct EnergyArgs {
+  int hidden, layers, latent, integrator;
+  float tau;
+  const float* params;
+  const float* scale;  // 6
+  int64_t n;
+  const float* strain;      // n x 6
+  const float* latent_in;   // n x L
+  const float* time_step;   // n
+  const float* anchors;     // 14: eq value, eq grad (6), neq value, neq strain grad (6); NULL = zeros
+  float* stress;            // n x 6
+  float* latent_out;        // n x L
+  float* rate;              // n x L
+  float* rate_dimless;      // n x L
+  float* scalars;           // 4 x n: dissipation, free energy, violation, energy increment
+  float* anchors_out;       // anchor mode: 14 outputs (point 0 of a zero input)
+};
+
+__global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs a) {
+  extern __shared__ float sm[];
+  const int hidden = a.hidden, layers = a.layers, L = a.latent;
+  const int ld = hidden + 1;
+  Smem s;
+  s.ld = ld;
+  s.x = sm;
+  s.gin = s.x + ER_TILE * ER_XLD;
+  s.h0 = s.gin + ER_TILE * ER_XLD;
+  s.h1 = s.h0 + ER_TILE * ld;
+  s.z = s.h1 + ER_TILE * ld;
+  float* eps = s.z + (int64_t)layers * ER_TILE * ld;  // [TILE][6] network strain
+  float* zin = eps + ER_TILE * 6;                      // [TILE][8] previous latent
+  float* zdl = zin + ER_TILE * 8;                      // [TILE][8] dimensionless rate
+  float* zc = zdl + ER_TILE * 8;                       // [TILE][8] candidate latent
+  float* geq = zc + ER_TILE * 8;                       // [TILE][6]
+  float* gpr = geq + ER_TILE * 6;                      // [TILE][16]
+  float* gca = gpr + ER_TILE * 16;                     // [TILE][16]
+  float* val = gca + ER_TILE * 16;                     // [3][TILE]: eq, previous, candidate values
+  const int t = threadIdx.x;
+  const int64_t p0 = (int64_t)blockIdx.x * ER_TILE;
+  const bool anchor_mode = a.anchors_out != nullptr;
+  const NetView eq{a.params, 6, 1};
+  const NetView neq{a.params + net_size(6, 1, hidden, layers), 6 + L, 1};
+  const NetView evo{neq.base + net_size(6 + L, 1, hidden, layers), 6 + L, L};
+  // per-point inputs (zeros beyond n and in anchor mode)
+  for (int i = t; i < ER_TILE * 8; i += ER_THREADS) {
+    const int p = i >> 3, c = i & 7;
+    const bool live = !anchor_mode && p0 + p < a.n;
+    if (c < 6) eps[p * 6 + c] = live ? a.strain[(p0 + p) * 6 + c] / a.scale[c] : 0.0f;
+    zin[i] = (live && c < L) ? a.latent_in[(p0 + p) * L + c] : 0.0f;
+  }
+  __syncthreads();
+  // 1. equilibrium potential and gradient at the network strain
+  for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
+    const int p = i / ER_XLD, c = i % ER_XLD;
+    s.x[i] = c < 6 ? eps[p * 6 + c] : 0.0f;
+  }
+  __syncthreads();
+  scalar_output(eq, hidden, layers, forward_hidden(eq, hidden, layers, s), ld, val);
+  input_gradient(eq, hidden, layers, s);
+  for (int i = t; i < ER_TILE * 6; i += ER_THREADS) geq[i] = s.gin[(i / 6) * ER_XLD + i % 6];
+  // 2. previous state [eps, z_n]: non-equilibrium potential and gradient, then the evolution net
+  for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
+    const int p = i / ER_XLD, c = i % ER_XLD;
+    s.x[i] = c < 6 ? eps[p * 6 + c] : (c < 6 + L ? zin[p * 8 + c - 6] : 0.0f);
+  }
+  __syncthreads();
+  scalar_output(neq, hidden, layers, forward_hidden(neq, hidden, layers, s), ld, val + ER_TILE);
+  input_gradient(neq, hidden, layers, s);
+  for (int i = t; i < ER_TILE * 16; i += ER_THREADS) gpr[i] = s.gin[(i / 16) * ER_XLD + (i % 16 < ER_XLD ? i % 16 : 0)];
+  __syncthreads();
+  {
+    const float* h = forward_hidden(evo, hidden, layers, s);  // s.x still holds the previous state
+    const float* wo = output_ptr(evo, hidden, layers);
+    const float* bo = wo + (int64_t)L * hidden;
+    for (int i = t; i < ER_TILE * L; i += ER_THREADS) {
+      const int p = i / L, o = i % L;
+      float v = bo[o];
+      for (int j = 0; j < hidden; ++j) v = fmaf(wo[(int64_t)o * hidden + j], h[p * ld + j], v);
+      zdl[p * 8 + o] = v;
+    }
+    __syncthreads();
+  }
+  // 3. forward-Euler candidate and the non-equilibrium potential there
+  for (int i = t; i < ER_TILE * 8; i += ER_THREADS) {
+    const int p = i >> 3, c = i & 7;
+    const bool live = !anchor_mode && p0 + p < a.n;
+    const float dt = live ? a.time_step[p0 + p] : 0.0f;
+    zc[i] = c < L ? zin[i] + (dt / a.tau) * zdl[i] : 0.0f;
+  }
+  __syncthreads();
+  for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
+    const int p = i / ER_XLD, c = i % ER_XLD;
+    s.x[i] = c < 6 ? eps[p * 6 + c] : (c < 6 + L ? zc[p * 8 + c - 6] : 0.0f);
+  }
+  __syncthreads();
+  scalar_output(neq, hidden, layers, forward_hidden(neq, hidden, layers, s), ld, val + 2 * ER_TILE);
+  input_gradient(neq, hidden, layers, s);
+  for (int i = t; i < ER_TILE * 16; i += ER_THREADS) gca[i] = s.gin[(i / 16) * ER_XLD + (i % 16 < ER_XLD ? i % 16 : 0)];
+  __syncthreads();
+  if (anchor_mode) {
+    if (t == 0) {
+      a.anchors_out[0] = val[0];
+      for (int c = 0; c < 6; ++c) a.anchors_out[1 + c] = geq[c];
+      a.anchors_out[7] = val[ER_TILE];
+      for (int c = 0; c < 6; ++c) a.anchors_out[8 + c] = gpr[c];
+    }
+    return;
+  }
+  // 4. anchored energies, stress, rates, dissipation (thread p owns point p)
+  if (t < ER_TILE && p0 + t < a.n) {
+    const int p = t;
+    const int64_t q = p0 + p;
+    float av_eq = 0.0f, av_neq = 0.0f, ag_eq[6], ag_neq[6];
+    for (int c = 0; c < 6; ++c) {
+      ag_eq[c] = a.anchors ? a.anchors[1 + c] : 0.0f;
+      ag_neq[c] = a.anchors ? a.anchors[8 + c] : 0.0f;
+    }
+    if (a.anchors) {
+      av_eq = a.anchors[0];
+      av_neq = a.anchors[7];
+    }
+    float xe = 0.0f, xn = 0.0f;
+    for (int c = 0; c < 6; ++c) {
+      xe += eps[p * 6 + c] * ag_eq[c];
+      xn += eps[p * 6 + c] * ag_neq[c];
+    }
+    const float equilibrium = val[p] - av_eq - xe;
+    const float prev_neq = val[ER_TILE + p] - av_neq - xn;
+    const float cand_neq = val[2 * ER_TILE + p] - av_neq - xn;
+    float diss = 0.0f;
+    for (int o = 0; o < L; ++o) {
+      const float r = zdl[p * 8 + o] / a.tau;
+      a.rate[q * L + o] = r;
+      a.rate_dimless[q * L + o] = zdl[p * 8 + o];
+      a.latent_out[q * L + o] = zc[p * 8 + o];
+      diss += gpr[p * 16 + 6 + o] * r;
+    }
+    diss = -diss;
+    const float* gresp = a.integrator == 1 ? gca + p * 16 : gpr + p * 16;
+    for (int c = 0; c < 6; ++c)
+      a.stress[q * 6 + c] = (geq[p * 6 + c] - ag_eq[c]) / a.scale[c] + (gresp[c] - ag_neq[c]) / a.scale[c];
+    a.scalars[q] = diss;
+    a.scalars[a.n + q] = equilibrium + (a.integrator == 1 ? cand_neq : prev_neq);
+    a.scalars[2 * a.n + q] = fmaxf(-diss, 0.0f);
+    a.scalars[3 * a.n + q] = cand_neq - prev_neq;
+  }
+}
+
+inline size_t energy_smem(int hidden, int layers) {
+  const size_t ld = (size_t)hidden + 1;
+  const size_t floats = (size_t)ER_TILE * ER_XLD * 2 + (size_t)ER_TILE * ld * (2 + layers) +
+                        (size_t)ER_TILE * (6 + 8 + 8 + 8 + 6 + 16 + 16) + 3 * ER_TILE;
+  return floats * sizeof(float);
+}
+
+int launch_energy(const cib_energy_rno* m, const EnergyArgs& a, int64_t blocks, cudaStream_t st) {
+  const size_t smem = energy_smem(m->hidden, m->layers);
+  if (smem > 200 * 1024) return CIB_ERANGE;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(energy_rno_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+        cudaSuccess)
+      return check_launch();
+    configured = true;
+  }
+  energy_rno_kernel<<<(unsigned)blocks, ER_THREADS, smem, st>>>(a);
+  return check_launch();
+}
+
+bool valid_model(const cib_energy_rno* m) {
+  return m && m->params && m->strain_scale && m->hidden >= 1 && m->hidden <= ER_THREADS && m->layers >= 1 &&
+         m->layers <= 8 && m->latent >= 1 && m->latent <= 8 && (m->integrator == 0 || m->integrator == 1) &&
+         m->reference_time_scale > 0.0;
+}
+
+EnergyArgs base_args(const cib_energy_rno* m) {
+  EnergyArgs a{};
+  a.hidden = m->hidden;
+  a.layers = m->layers;
+  a.latent = m->latent;
+  a.integrator = m->integrator;
+  a.tau = (float)m->reference_time_scale;
+  a.params = m->params;
+  a.scale = m->strain_scale;
+  return a;
+}
+
+}  // namespace
+}  // namespace cib
+
+using namespace cib;
+
+extern "C" int64_t cib_energy_rno_param_count(int32_t hidden, int32_t layers, int32_t latent) {
+  if (hidden < 1 || layers < 1 || latent < 1) return -1;
+  return net_size(6, 1, hidden, layers) + net_size(6 + latent, 1, hidden, layers) +
+         net_size(6 + latent, latent, hidden, layers);
+}
+
+extern "C" int cib_energy_rno_anchors(const cib_energy_rno* model, float* anchors, void* stream) {
+  if (!valid_model(model) || !anchors) return CIB_EINVAL;
+  EnergyArgs a = base_args(model);
+  a.n = 1;
+  a.anchors_out = anchors;
+  return launch_energy(model, a, 1, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int cib_energy_rno_update(const cib_energy_rno* model, int64_t n, const float* strain, const float* latent,
+                                     const float* time_step, const float* anchors, float* stress, float* latent_out,
+                                     float* state_rate, float* dimensionless_rate, float* scalars, void* stream) {
+  if (!valid_model(model) || n < 0 || !strain || !latent || !time_step || !stress || !latent_out || !state_rate ||
+      !dimensionless_rate || !scalars)
+    return CIB_EINVAL;
+  if (n == 0) return CIB_OK;
+  EnergyArgs a = base_args(model);
+  a.n = n;
+  a.strain = strain;
+  a.latent_in = latent;
+  a.time_step = time_step;
+  a.anchors = anchors;
+  a.stress = stress;
+  a.latent_out = latent_out;
+  a.rate = state_rate;
+  a.rate_dimless = dimensionless_rate;
+  a.scalars = scalars;
+  return launch_energy(model, a, (n + ER_TILE - 1) / ER_TILE, reinterpret_cast<cudaStream_t>(stream));
+}

@@ -482,6 +482,42 @@ int cib_csr_pcg(int64_t n, const int64_t* indptr, const int64_t* indices, const 
                 double* p, double* q, double* work, double rtol, int32_t maxit, int32_t check_every, int32_t* status,
                 int32_t* iterations, double* relative_residual, void* stream);
 
+/* --- Energy-based RVE-RNO (the reference's surrogate family) ------------------------------
+ * FP32 update of src/concrete_impact/nn/models/rve_rno.py:334-418 (EnergyDissipationRVERNO,
+ * direct_rate evolution) with the input gradients of ScalarMLP.value_and_input_gradient
+ * (:110-129).  Three SiLU networks of `layers` hidden layers of width `hidden` (<= 128):
+ * equilibrium potential (6 inputs), non-equilibrium potential (6 + latent inputs), state
+ * evolution (6 + latent -> latent).  `params` packs, network after network in that order,
+ * for every hidden layer l: W [hidden][in_l] (torch Linear layout), its transpose
+ * Wt [in_l][hidden], bias [hidden]; then the output weights [out][hidden] and output bias
+ * [out] (zeros for the two potentials).  integrator 1 = current_state_stress_forward_euler
+ * (stress from the forward-Euler candidate state), 0 = cs_semi_implicit_forward_euler
+ * (stress from the previous state).  latent <= 8. */
+typedef struct cib_energy_rno {
+  int32_t hidden;
+  int32_t layers;
+  int32_t latent;
+  int32_t integrator;
+  double reference_time_scale;
+  const float* params;       /* cib_energy_rno_param_count floats (device) */
+  const float* strain_scale; /* 6 floats (device): network strain = strain / scale */
+} cib_energy_rno;
+
+/* Length of `params` for a model shape (-1 for an invalid shape); host only. */
+int64_t cib_energy_rno_param_count(int32_t hidden, int32_t layers, int32_t latent);
+
+/* Zero-state energy anchors (prepare_energy_anchors, rve_rno.py:227-247) into 14 floats:
+ * equilibrium value, its strain gradient (6), non-equilibrium value, its strain gradient (6). */
+int cib_energy_rno_anchors(const cib_energy_rno* model, float* anchors, void* stream);
+
+/* One update of n points (update_batch without tangent, rve_rno.py:249-313): strain (n,6),
+ * latent (n,latent), time_step (n), anchors (14, NULL = zeros) -> stress (n,6), latent_out,
+ * state_rate and dimensionless_rate (n,latent), scalars (4 rows of n: dissipation, free
+ * energy, thermodynamic violation, non-equilibrium energy increment).  All FP32, device. */
+int cib_energy_rno_update(const cib_energy_rno* model, int64_t n, const float* strain, const float* latent,
+                          const float* time_step, const float* anchors, float* stress, float* latent_out,
+                          float* state_rate, float* dimensionless_rate, float* scalars, void* stream);
+
 /* Error gate of the surrogate at n macro points (no reference counterpart; the reference's
  * deployment adapter, src/concrete_impact/nn/deployment.py:68-165, has no input gate).
  * prepare: strain_n = strain / strain_scale, rate_n = rate / rate_scale (fp32, n x 6),

@@ -416,7 +416,70 @@ def make_ogrid_cases():
     return {"rve_ogrid_cylinder": (arrays, meta)}
 
 
-GROUPS = ("j2", "rve", "newmark", "ogrid")
+def make_rno_energy_cases(src: str):
+    """The reference's trained energy-based RVE-RNO (artifacts/rve_rno/c48_v2_liu_direct):
+    its weights, energy anchors and a 12-step rollout of update_batch (FP32, CPU) for 128
+    points along seeded linear strain ramps, with the trained integrator
+    (current_state_stress_forward_euler) and, on the last step's inputs, the
+    cs_semi_implicit_forward_euler branch."""
+    import torch
+
+    from concrete_impact.nn.config import RVERNOModelConfig
+    from concrete_impact.nn.models.rve_rno import EnergyDissipationRVERNO
+
+    artifact = Path(src).parent / "artifacts" / "rve_rno" / "c48_v2_liu_direct"
+    metadata = json.loads((artifact / "artifact_metadata.json").read_text())
+    fields = ("integrator", "evolution", "reference_time_scale", "latent_dimension", "hidden_size", "hidden_layers",
+              "activation", "time_representation", "dtype")  # fmt: skip
+    spec = {k: metadata[k] for k in fields}
+    spec.update(family=metadata["model_family"], device="cpu")
+    state_dict = torch.load(artifact / "best_model.pt", map_location="cpu", weights_only=True)["model_state_dict"]
+    models = {}
+    for integrator in ("current_state_stress_forward_euler", "cs_semi_implicit_forward_euler"):
+        model = EnergyDissipationRVERNO(RVERNOModelConfig(**dict(spec, integrator=integrator)))
+        model.load_state_dict(state_dict, strict=True)
+        model.eval()
+        models[integrator] = model
+    rng = np.random.default_rng(91000)
+    n, steps = 128, 12
+    norm = metadata["normalization"]["macro_strain"]
+    target = np.asarray(norm["mean"]) + np.asarray(norm["rms_scale"]) * rng.standard_normal((n, 6))
+    dt = np.exp(rng.uniform(np.log(1.0e-4), np.log(2.0e-3), size=n))
+    arrays = {f"w__{k}": v.numpy() for k, v in state_dict.items()}
+    main = models["current_state_stress_forward_euler"]
+    anchors = main.prepare_energy_anchors()
+    arrays.update(anchor_equilibrium_value=anchors.equilibrium_value.detach().numpy(),
+                  anchor_equilibrium_gradient=anchors.equilibrium_strain_gradient.detach().numpy(),
+                  anchor_nonequilibrium_value=anchors.nonequilibrium_value.detach().numpy(),
+                  anchor_nonequilibrium_gradient=anchors.nonequilibrium_strain_gradient.detach().numpy())  # fmt: skip
+    latent = torch.zeros((n, 6), dtype=torch.float32)
+    keys = ("stress", "latent_state", "state_rate", "dimensionless_state_rate", "dissipation", "free_energy",
+            "thermodynamic_violation", "nonequilibrium_energy_increment")  # fmt: skip
+    out = {k: [] for k in keys}
+    strains, latents_in, semi = [], [], {k: [] for k in keys}
+    with torch.no_grad():
+        for step in range(1, steps + 1):
+            strain = torch.as_tensor(target * step / steps, dtype=torch.float32)
+            time_step = torch.as_tensor(dt, dtype=torch.float32)
+            strains.append(strain.numpy())
+            latents_in.append(latent.numpy())
+            res = main.update_batch(strain, latent, time_step, anchors)
+            for k in keys:
+                out[k].append(getattr(res, k).numpy())
+            if step == steps:  # the other integrator on the last step's inputs
+                other = models["cs_semi_implicit_forward_euler"].update_batch(strain, latent, time_step, anchors)
+                for k in keys:
+                    semi[k].append(getattr(other, k).numpy())
+            latent = res.latent_state
+    arrays.update(strain=np.stack(strains), latent_in=np.stack(latents_in), time_step=dt.astype(np.float32))
+    arrays.update({f"out__{k}": np.stack(v) for k, v in out.items()})
+    arrays.update({f"semi__{k}": np.stack(v) for k, v in semi.items()})
+    meta = {"model": spec, "points": n, "steps": steps, "seed": 91000, "artifact": "artifacts/rve_rno/c48_v2_liu_direct",
+            "accepted_time_step_range": metadata["accepted_time_step_range"]}  # fmt: skip
+    return {"rno_energy_c48": (arrays, meta)}
+
+
+GROUPS = ("j2", "rve", "newmark", "ogrid", "rno_energy")
 
 
 def main() -> None:
@@ -440,6 +503,8 @@ def main() -> None:
         cases.update(make_newmark_cases())
     if "ogrid" in groups:
         cases.update(make_ogrid_cases())
+    if "rno_energy" in groups:
+        cases.update(make_rno_energy_cases(args.reference))
     path = HERE / "manifest.json"
     manifest = json.loads(path.read_text()) if path.exists() and args.only else {}
     for name, (arrays, meta) in cases.items():
