@@ -10,7 +10,7 @@ tangent=True).  Headline precision is float64 (the reference's); the float32 var
 the method is reported alongside.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload return_map|rve_path|rve_batch|rno_train|fe2|implicit_fe2|rve_ogrid]
+                    [--workload return_map|rve_path|rve_batch|rno_train|fe2|implicit_fe2|rve_ogrid|rno_energy]
 
 Under torchrun each rank updates its own batch of the same size (independent points:
 weak scaling, no collective on the data path); rank 0 prints the line.  The other
@@ -42,7 +42,7 @@ WORKLOAD = "isolated batched return map, 16,777,216 GP SoA, FP64 state, tangent 
 FALLBACK_HBM_GBS = 6650.0
 # (timed steps, warm-up steps) per workload when not given on the command line
 WORKLOAD_DEFAULTS = {"return_map": (200, 5), "rve_path": (100, 3), "rve_batch": (5, 3), "rno_train": (300, 1),
-                     "fe2": (5000, 5), "implicit_fe2": (10, 3), "rve_ogrid": (20, 3)}
+                     "fe2": (5000, 5), "implicit_fe2": (10, 3), "rve_ogrid": (20, 3), "rno_energy": (50, 3)}
 
 
 def parse_args() -> argparse.Namespace:

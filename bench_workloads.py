@@ -16,6 +16,8 @@
   against all-direct FP64 FE^2 on a 64x2x2 bar.
 * rve_ogrid -- the cylindrical O-grid two-phase RVE (2,560 general Hex8 elements) along a
   20-step compression path; metric: accepted RVE steps/s through solve_prescribed_rve_path.
+* rno_energy -- the reference's trained energy-based RVE-RNO at 131,072 macro points, 50
+  chained updates (weights from tests/golden/rno_energy_c48.npz); metric: point-updates/s.
 * implicit_fe2 -- implicit Newmark FE^2 (solve_material_implicit_newmark) on a 16x4x4 bar
   with an 8^3 concrete RVE (FP64) at each of the 2,048 macro points; metric: accepted macro
   steps/s through the public call (host arrays in and out), RVE solves/s beside it.
@@ -453,6 +455,74 @@ def run_rve_ogrid(args: argparse.Namespace) -> None:
 
 
 # ---------------------------------------------------------------------------------------
+# rno_energy
+
+
+def _energy_case():
+    from pathlib import Path
+
+    from concrete_impact_b200.energy_rno import RVERNOModelConfig
+
+    here = Path(__file__).resolve().parent / "tests" / "golden"
+    meta = json.loads((here / "manifest.json").read_text())["rno_energy_c48"]
+    with np.load(here / "rno_energy_c48.npz") as data:
+        state_dict = {k[3:]: data[k] for k in data.files if k.startswith("w__")}
+    return state_dict, RVERNOModelConfig(**{k: v for k, v in meta["model"].items() if k != "device"})
+
+
+def _rno_energy_cpu(points: int = 2048) -> dict:
+    """The NumPy oracle (float64, the reference's update) on a bounded sample of points."""
+    from oracle import rno_energy as oe
+
+    state_dict, cfg = _energy_case()
+    rng = np.random.default_rng(7)
+    strain = 5.0e-3 * rng.standard_normal((points, 6))
+    latent = np.zeros((points, 6))
+    anchor = oe.anchors(state_dict, 6)
+    from threadpoolctl import threadpool_limits
+
+    with threadpool_limits(1):
+        t0 = time.perf_counter()
+        oe.update(state_dict, strain, latent, np.full(points, 1.0e-4), cfg.reference_time_scale, cfg.integrator,
+                  anchor=anchor)  # fmt: skip
+        seconds = time.perf_counter() - t0
+    return {"value": points / seconds, "unit": "point-updates/s", "cores": 1, "kind": "port",
+            "sample": f"NumPy oracle (float64, one BLAS thread), one update of {points} points ({seconds:.2f} s)"}  # fmt: skip
+
+
+def run_rno_energy(args: argparse.Namespace) -> None:
+    import torch
+
+    from bench import ClockSampler
+    from concrete_impact_b200.benchmarks import energy_rno_workload
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    state_dict, cfg = _energy_case()
+    with ClockSampler(local) as clocks:
+        out = energy_rno_workload(state_dict, cfg, steps=args.steps, warmup=args.warmup)
+    if rank != 0:
+        return
+    seconds = out["ms"] / 1e3
+    value = out["points"] * out["steps"] / seconds
+    achieved = value * out["flop_per_point"] / 1e12
+    line = _line(args, "energy-based RVE-RNO point-updates/s (the reference's trained c48 model, 131,072 macro "
+                       "points, FP32)", value, "point-updates/s",
+                 "rno_energy: EnergyDissipationRVERNO 4x128 SiLU, latent 6, direct_rate, current-state integrator",
+                 {"ms_per_step": out["ms"] / max(out["steps"], 1), "dtype": "f32",
+                  "flop_per_point_update": out["flop_per_point"],
+                  "roofline": {"bound": "fp32 cuda cores", "achieved": achieved, "peak": None, "unit": "TFLOP/s",
+                               "frac": None, "traffic": None,
+                               "note": "FP32 SIMT kernel; no measured FP32 CUDA-core peak for the denominator"},
+                  "gpu_launches": out["launches"],
+                  "e2e": {"value": value, "unit": "point-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                          "path": "update_batch on device-resident strains and latent states"},
+                  "clocks": clocks.summary(), "cpu_baseline": None if args.no_cpu_baseline else _rno_energy_cpu()})  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
 # implicit_fe2
 
 IMPLICIT_FE2_POINTS = 2048
@@ -524,8 +594,10 @@ def run_reference(args: argparse.Namespace) -> None:
     """``--impl reference``: the oracle alone on the workload's CPU sample (rank 0)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    if args.workload in ("rno_train", "fe2", "implicit_fe2", "rve_ogrid"):
-        if args.workload == "implicit_fe2":
+    if args.workload in ("rno_train", "fe2", "implicit_fe2", "rve_ogrid", "rno_energy"):
+        if args.workload == "rno_energy":
+            c = _rno_energy_cpu()
+        elif args.workload == "implicit_fe2":
             c = _implicit_fe2_cpu(float(IMPLICIT_FE2_POINTS * IMPLICIT_FE2_EVALUATIONS))
         elif args.workload == "rve_ogrid":
             c = _rve_ogrid_cpu()
@@ -536,7 +608,8 @@ def run_reference(args: argparse.Namespace) -> None:
                   "fe2": "direct FE2 macro steps/s (oracle RVE solves on the host)",
                   "implicit_fe2": "implicit FE2 macro steps/s (oracle RVE solves with effective tangents on the host, "
                                   f"{IMPLICIT_FE2_EVALUATIONS} material evaluations per step)",
-                  "rve_ogrid": "accepted RVE steps/s (general-mesh RVE oracle, cylindrical O-grid)"}[args.workload]  # fmt: skip
+                  "rve_ogrid": "accepted RVE steps/s (general-mesh RVE oracle, cylindrical O-grid)",
+                  "rno_energy": "energy-based RVE-RNO point-updates/s (NumPy oracle on the host)"}[args.workload]  # fmt: skip
         line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32" if args.workload == "rno_train" else "f64", "data": "synthetic",
@@ -609,5 +682,7 @@ def run(args: argparse.Namespace) -> None:
         run_implicit_fe2(args)
     elif args.workload == "rve_ogrid":
         run_rve_ogrid(args)
+    elif args.workload == "rno_energy":
+        run_rno_energy(args)
     else:
         raise SystemExit(f"unknown workload {args.workload}")

@@ -20,6 +20,9 @@ rve_heterogeneous.py, dynamic_viscoplastic.py) for the concrete RVE of this pack
 * ``ogrid_rve_path_workload`` -- the cylindrical O-grid two-phase RVE (32 circumferential,
   8 radial, 8 axial divisions: 2,560 elements, 30 % inclusion) along a 20-step compression
   path through solve_prescribed_rve_path (general-mesh device path, FP64).
+* ``energy_rno_workload`` -- the reference's trained energy-based RVE-RNO (4 x 128 SiLU
+  networks) at the 131,072 macro points of the 64 x 16 x 16 bar: one update_batch per step
+  along seeded strain ramps, FP32.
 * ``implicit_fe2_workload`` -- implicit FE^2 through solve_material_implicit_newmark: a
   16 x 4 x 4 Hex8 bar (0.01 m elements, 2,048 macro points) with an 8^3 concrete RVE (FP64)
   at every point, average-acceleration Newmark at 5 us under a half-sine 40 MPa pulse.
@@ -543,3 +546,44 @@ def ogrid_rve_path_workload(steps: int = 20, warmup: int = 3) -> dict:
             "evaluations": 8 * int(model.elements.shape[0]) * (sum(newton) + len(newton)),
             "launches": _native.LAUNCHED[0] - calls0, "macro_stress": [np.asarray(r.macro_stress).tolist() for r in result.responses],
             "times": times, "strains": strains, "mesh": mesh}  # fmt: skip
+
+
+
+def energy_rno_flop(hidden: int = 128, layers: int = 4, latent: int = 6) -> int:
+    """Multiply-adds x 2 of one update: four network passes (equilibrium, non-equilibrium at
+    the previous and candidate states, evolution) and three input-gradient passes."""
+    def hidden_macs(n_in: int) -> int:
+        return n_in * hidden + (layers - 1) * hidden * hidden
+
+    forward = hidden_macs(6) + hidden + 2 * (hidden_macs(6 + latent) + hidden) + hidden_macs(6 + latent) + latent * hidden
+    backward = hidden_macs(6) + 2 * hidden_macs(6 + latent)
+    return 2 * (forward + backward)
+
+
+def energy_rno_workload(state_dict: dict, config, points: int = 131072, steps: int = 50, warmup: int = 3) -> dict:
+    """Update throughput of the energy-based RVE-RNO at ``points`` macro points: ``steps``
+    chained updates along seeded strain ramps (dt 1e-4 s), CUDA-event timed."""
+    from .energy_rno import EnergyDissipationRVERNO
+
+    model = EnergyDissipationRVERNO(config)
+    model.load_state_dict(state_dict)
+    anchors = model.prepare_energy_anchors()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    target = 5.0e-3 * torch.randn((points, 6), generator=g, device="cuda", dtype=torch.float32)
+    dt = torch.full((points,), 1.0e-4, dtype=torch.float32, device="cuda")
+    latent = model.initial_state_batch(points)
+    for k in range(warmup):
+        latent = model.update_batch(target * (k + 1) / (warmup + steps), latent, dt, anchors).latent_state
+    calls0 = _native.LAUNCHED[0]
+    box = {"z": latent}
+
+    def run() -> None:
+        z = box["z"]
+        for k in range(steps):
+            z = model.update_batch(target * (warmup + k + 1) / (warmup + steps), z, dt, anchors).latent_state
+        box["z"] = z
+
+    ms = _elapsed_ms(run)
+    return {"ms": ms, "steps": steps, "points": points, "launches": _native.LAUNCHED[0] - calls0,
+            "flop_per_point": energy_rno_flop(config.hidden_size, config.hidden_layers, config.latent_dimension),
+            "latent_abs_max": float(box["z"].abs().max())}  # fmt: skip
