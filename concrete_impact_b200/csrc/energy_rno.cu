@@ -10,11 +10,11 @@
 // three hand-written input-gradient passes of 6/12 -> hidden^layers -> 1 (or 6) networks.
 //
 // One CTA of 128 threads per tile of 32 points.  Forward layers: thread j owns hidden unit j
-// and keeps the 32 points' accumulators in registers; the layer's input rows sit in shared
-// memory (broadcast reads) and the transposed weights are read along j (coalesced).
-// Input-gradient layers: thread k owns input k and reads the weights along k (coalesced).
-// Pre-activations of every layer stay in shared memory for the backward pass; shared rows
-// are padded to hidden + 1 floats so that per-point column reads hit distinct banks.
+// and keeps the 32 points' accumulators in registers; the layer's input sits in shared
+// memory feature-major (the 32 points of a feature read as eight float4 broadcasts) and the
+// transposed weights are read along j (coalesced).  Input-gradient layers: thread k owns
+// input k and reads the weights along k (coalesced).  Pre-activations of every layer stay in
+// shared memory for the backward pass.
 // Everything is FP32 like the reference model (its dtype float32); no waits besides
 // __syncthreads.
 #include <cuda_runtime.h>
@@ -75,26 +75,38 @@ __device__ __forceinline__ float silu_prime(float z) {
   return s * (1.0f + z * (1.0f - s));
 }
 
+// Shared buffers are feature-major, one row of ER_TILE floats per feature (input, hidden
+// unit), so a layer reads the 32 points of one feature as eight float4 broadcasts.  The
+// float4 groups of row r are XOR-swizzled by r & 7: a thread writing its own row and a
+// thread reading one point across rows both hit 32 distinct banks.
+__device__ __forceinline__ int sw(int row, int p) { return row * ER_TILE + ((((p >> 2) ^ (row & 7)) << 2) | (p & 3)); }
+
+__device__ __forceinline__ float4* grp(float* buf, int row, int g) {
+  return reinterpret_cast<float4*>(buf + row * ER_TILE + ((g ^ (row & 7)) << 2));
+}
+
+__device__ __forceinline__ const float4* grp(const float* buf, int row, int g) {
+  return reinterpret_cast<const float4*>(buf + row * ER_TILE + ((g ^ (row & 7)) << 2));
+}
+
 struct Smem {
-  float* x;     // [TILE][XLD] network input
-  float* z;     // [layers][TILE][LD] pre-activations
-  float* h0;    // [TILE][LD]
-  float* h1;    // [TILE][LD]
-  float* gin;   // [TILE][XLD] input gradient
-  int ld;
+  float* x;    // [XLD rows][TILE] network input
+  float* gin;  // [XLD rows][TILE] input gradient
+  float* h0;   // [hidden rows][TILE]
+  float* h1;   // [hidden rows][TILE]
+  float* z;    // [layers][hidden rows][TILE] pre-activations
 };
 
 // Forward pass of the hidden layers; returns the buffer holding the last activation.
 __device__ float* forward_hidden(const NetView& n, int hidden, int layers, const Smem& s) {
   const int j = threadIdx.x;
   const float* hin = s.x;
-  int ldin = ER_XLD;
   float* hout = s.h0;
   for (int l = 0; l < layers; ++l) {
     const float *W, *Wt, *b;
     layer_ptrs(n, hidden, l, &W, &Wt, &b);
     const int in_l = l == 0 ? n.in : hidden;
-    float* zl = s.z + (int64_t)l * ER_TILE * s.ld;
+    float* zl = s.z + (int64_t)l * hidden * ER_TILE;
     if (j < hidden) {
       float acc[ER_TILE];
       const float bj = b[j];
@@ -103,47 +115,56 @@ __device__ float* forward_hidden(const NetView& n, int hidden, int layers, const
       for (int k = 0; k < in_l; ++k) {
         const float w = Wt[(int64_t)k * hidden + j];
 #pragma unroll
-        for (int p = 0; p < ER_TILE; ++p) acc[p] = fmaf(w, hin[p * ldin + k], acc[p]);
+        for (int g = 0; g < ER_TILE / 4; ++g) {
+          const float4 v = *grp(hin, k, g);
+          acc[4 * g] = fmaf(w, v.x, acc[4 * g]);
+          acc[4 * g + 1] = fmaf(w, v.y, acc[4 * g + 1]);
+          acc[4 * g + 2] = fmaf(w, v.z, acc[4 * g + 2]);
+          acc[4 * g + 3] = fmaf(w, v.w, acc[4 * g + 3]);
+        }
       }
 #pragma unroll
-      for (int p = 0; p < ER_TILE; ++p) {
-        zl[p * s.ld + j] = acc[p];
-        hout[p * s.ld + j] = silu(acc[p]);
+      for (int g = 0; g < ER_TILE / 4; ++g) {
+        *grp(zl, j, g) = make_float4(acc[4 * g], acc[4 * g + 1], acc[4 * g + 2], acc[4 * g + 3]);
+        *grp(hout, j, g) = make_float4(silu(acc[4 * g]), silu(acc[4 * g + 1]), silu(acc[4 * g + 2]),
+                                       silu(acc[4 * g + 3]));
       }
     }
     __syncthreads();
     hin = hout;
-    ldin = s.ld;
     hout = (hout == s.h0) ? s.h1 : s.h0;
   }
   return const_cast<float*>(hin);
 }
 
 // Scalar potential value per point (threads p < TILE) into value[p].
-__device__ void scalar_output(const NetView& n, int hidden, int layers, const float* h, int ld, float* value) {
+__device__ void scalar_output(const NetView& n, int hidden, int layers, const float* h, float* value) {
   const float* wo = output_ptr(n, hidden, layers);
   const int p = threadIdx.x;
   if (p < ER_TILE) {
     float v = 0.0f;
-    for (int j = 0; j < hidden; ++j) v = fmaf(wo[j], h[p * ld + j], v);
+    for (int j = 0; j < hidden; ++j) v = fmaf(wo[j], h[sw(j, p)], v);
     value[p] = v;
   }
   __syncthreads();
 }
 
-// Input gradient of a scalar network into s.gin[p][0..in) (pre-activations in s.z).
+// Input gradient of a scalar network into rows 0..in of s.gin (pre-activations in s.z).
 __device__ void input_gradient(const NetView& n, int hidden, int layers, const Smem& s) {
   const float* wo = output_ptr(n, hidden, layers);
   const int t = threadIdx.x;
-  float* g = s.h0;  // gradient wrt the activation of layer l (rows TILE x ld)
+  float* g = s.h0;  // gradient wrt the activation of layer l
   float* d = s.h1;  // gradient wrt the pre-activation of layer l
   for (int l = layers - 1; l >= 0; --l) {
-    const float* zl = s.z + (int64_t)l * ER_TILE * s.ld;
+    const float* zl = s.z + (int64_t)l * hidden * ER_TILE;
     if (t < hidden) {
-#pragma unroll 4
-      for (int p = 0; p < ER_TILE; ++p) {
-        const float gv = (l == layers - 1) ? wo[t] : g[p * s.ld + t];
-        d[p * s.ld + t] = gv * silu_prime(zl[p * s.ld + t]);
+      const float wt = wo[t];
+#pragma unroll
+      for (int q = 0; q < ER_TILE / 4; ++q) {
+        const float4 zz = *grp(zl, t, q);
+        const float4 gv = (l == layers - 1) ? make_float4(wt, wt, wt, wt) : *grp(g, t, q);
+        *grp(d, t, q) = make_float4(gv.x * silu_prime(zz.x), gv.y * silu_prime(zz.y), gv.z * silu_prime(zz.z),
+                                    gv.w * silu_prime(zz.w));
       }
     }
     __syncthreads();
@@ -151,7 +172,6 @@ __device__ void input_gradient(const NetView& n, int hidden, int layers, const S
     layer_ptrs(n, hidden, l, &W, &Wt, &b);
     const int in_l = l == 0 ? n.in : hidden;
     float* dst = l == 0 ? s.gin : g;
-    const int lddst = l == 0 ? ER_XLD : s.ld;
     if (t < in_l) {
       float acc[ER_TILE];
 #pragma unroll
@@ -159,10 +179,17 @@ __device__ void input_gradient(const NetView& n, int hidden, int layers, const S
       for (int jj = 0; jj < hidden; ++jj) {
         const float w = W[(int64_t)jj * in_l + t];
 #pragma unroll
-        for (int p = 0; p < ER_TILE; ++p) acc[p] = fmaf(d[p * s.ld + jj], w, acc[p]);
+        for (int q = 0; q < ER_TILE / 4; ++q) {
+          const float4 v = *grp(d, jj, q);
+          acc[4 * q] = fmaf(v.x, w, acc[4 * q]);
+          acc[4 * q + 1] = fmaf(v.y, w, acc[4 * q + 1]);
+          acc[4 * q + 2] = fmaf(v.z, w, acc[4 * q + 2]);
+          acc[4 * q + 3] = fmaf(v.w, w, acc[4 * q + 3]);
+        }
       }
 #pragma unroll
-      for (int p = 0; p < ER_TILE; ++p) dst[p * lddst + t] = acc[p];
+      for (int q = 0; q < ER_TILE / 4; ++q)
+        *grp(dst, t, q) = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
     }
     __syncthreads();
   }
@@ -189,15 +216,13 @@ struct EnergyArgs {
 __global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs a) {
   extern __shared__ float sm[];
   const int hidden = a.hidden, layers = a.layers, L = a.latent;
-  const int ld = hidden + 1;
   Smem s;
-  s.ld = ld;
   s.x = sm;
   s.gin = s.x + ER_TILE * ER_XLD;
   s.h0 = s.gin + ER_TILE * ER_XLD;
-  s.h1 = s.h0 + ER_TILE * ld;
-  s.z = s.h1 + ER_TILE * ld;
-  float* eps = s.z + (int64_t)layers * ER_TILE * ld;  // [TILE][6] network strain
+  s.h1 = s.h0 + ER_TILE * hidden;
+  s.z = s.h1 + ER_TILE * hidden;
+  float* eps = s.z + (int64_t)layers * ER_TILE * hidden;  // [TILE][6] network strain
   float* zin = eps + ER_TILE * 6;                      // [TILE][8] previous latent
   float* zdl = zin + ER_TILE * 8;                      // [TILE][8] dimensionless rate
   float* zc = zdl + ER_TILE * 8;                       // [TILE][8] candidate latent
@@ -222,21 +247,21 @@ __global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs
   // 1. equilibrium potential and gradient at the network strain
   for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
     const int p = i / ER_XLD, c = i % ER_XLD;
-    s.x[i] = c < 6 ? eps[p * 6 + c] : 0.0f;
+    s.x[sw(c, p)] = c < 6 ? eps[p * 6 + c] : 0.0f;
   }
   __syncthreads();
-  scalar_output(eq, hidden, layers, forward_hidden(eq, hidden, layers, s), ld, val);
+  scalar_output(eq, hidden, layers, forward_hidden(eq, hidden, layers, s), val);
   input_gradient(eq, hidden, layers, s);
-  for (int i = t; i < ER_TILE * 6; i += ER_THREADS) geq[i] = s.gin[(i / 6) * ER_XLD + i % 6];
+  for (int i = t; i < ER_TILE * 6; i += ER_THREADS) geq[i] = s.gin[sw(i % 6, i / 6)];
   // 2. previous state [eps, z_n]: non-equilibrium potential and gradient, then the evolution net
   for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
     const int p = i / ER_XLD, c = i % ER_XLD;
-    s.x[i] = c < 6 ? eps[p * 6 + c] : (c < 6 + L ? zin[p * 8 + c - 6] : 0.0f);
+    s.x[sw(c, p)] = c < 6 ? eps[p * 6 + c] : (c < 6 + L ? zin[p * 8 + c - 6] : 0.0f);
   }
   __syncthreads();
-  scalar_output(neq, hidden, layers, forward_hidden(neq, hidden, layers, s), ld, val + ER_TILE);
+  scalar_output(neq, hidden, layers, forward_hidden(neq, hidden, layers, s), val + ER_TILE);
   input_gradient(neq, hidden, layers, s);
-  for (int i = t; i < ER_TILE * 16; i += ER_THREADS) gpr[i] = s.gin[(i / 16) * ER_XLD + (i % 16 < ER_XLD ? i % 16 : 0)];
+  for (int i = t; i < ER_TILE * 16; i += ER_THREADS) gpr[i] = s.gin[sw(i % 16, i / 16)];
   __syncthreads();
   {
     const float* h = forward_hidden(evo, hidden, layers, s);  // s.x still holds the previous state
@@ -245,7 +270,7 @@ __global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs
     for (int i = t; i < ER_TILE * L; i += ER_THREADS) {
       const int p = i / L, o = i % L;
       float v = bo[o];
-      for (int j = 0; j < hidden; ++j) v = fmaf(wo[(int64_t)o * hidden + j], h[p * ld + j], v);
+      for (int j = 0; j < hidden; ++j) v = fmaf(wo[(int64_t)o * hidden + j], h[sw(j, p)], v);
       zdl[p * 8 + o] = v;
     }
     __syncthreads();
@@ -260,12 +285,12 @@ __global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs
   __syncthreads();
   for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
     const int p = i / ER_XLD, c = i % ER_XLD;
-    s.x[i] = c < 6 ? eps[p * 6 + c] : (c < 6 + L ? zc[p * 8 + c - 6] : 0.0f);
+    s.x[sw(c, p)] = c < 6 ? eps[p * 6 + c] : (c < 6 + L ? zc[p * 8 + c - 6] : 0.0f);
   }
   __syncthreads();
-  scalar_output(neq, hidden, layers, forward_hidden(neq, hidden, layers, s), ld, val + 2 * ER_TILE);
+  scalar_output(neq, hidden, layers, forward_hidden(neq, hidden, layers, s), val + 2 * ER_TILE);
   input_gradient(neq, hidden, layers, s);
-  for (int i = t; i < ER_TILE * 16; i += ER_THREADS) gca[i] = s.gin[(i / 16) * ER_XLD + (i % 16 < ER_XLD ? i % 16 : 0)];
+  for (int i = t; i < ER_TILE * 16; i += ER_THREADS) gca[i] = s.gin[sw(i % 16, i / 16)];
   __syncthreads();
   if (anchor_mode) {
     if (t == 0) {
@@ -317,8 +342,7 @@ __global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs
 }
 
 inline size_t energy_smem(int hidden, int layers) {
-  const size_t ld = (size_t)hidden + 1;
-  const size_t floats = (size_t)ER_TILE * ER_XLD * 2 + (size_t)ER_TILE * ld * (2 + layers) +
+  const size_t floats = (size_t)ER_TILE * ER_XLD * 2 + (size_t)ER_TILE * hidden * (2 + layers) +
                         (size_t)ER_TILE * (6 + 8 + 8 + 8 + 6 + 16 + 16) + 3 * ER_TILE;
   return floats * sizeof(float);
 }
