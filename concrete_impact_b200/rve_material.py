@@ -4,7 +4,9 @@ Drop-in for the reference's RVEHomogenizedMaterial (src/fem/rve/material.py:40-2
 same state keys (``rve_macro_strain``, ``rve_fluctuation_dofs``, ``rve_material__<key>``),
 outputs and macro diagnostics.  Where the reference solves the macro points' RVEs one by
 one (serially or in a process pool), here every macro point of an update call is one RVE
-of a single device batch: one launch per kernel advances all of them together.
+of a single device batch: one launch per kernel advances all of them together.  RVEs on
+general meshes (the cylindrical O-grid RVE) are solved point by point with the
+general-mesh device path, as the reference's serial loop (material.py:113-215).
 """
 
 from __future__ import annotations
@@ -102,6 +104,10 @@ class RVEHomogenizedMaterial:
         requirements: MaterialResponseRequirements = DEFAULT_RESPONSE_REQUIREMENTS,
     ) -> MaterialPointResponse:
         """Solve the RVEs of every macro integration point in one device batch."""
+        from .rve import is_structured_box
+
+        if not is_structured_box(self.model):
+            return self._update_general(request, state, requirements)
         n = int(request.strains.shape[0])
         io = _Io(request.strains)
         batch = self._batch(n)
@@ -196,9 +202,96 @@ class RVEHomogenizedMaterial:
                 out[f"phase_{pname}__maximum_equivalent_plastic_strain"] = sums[:, RS_QMAX + i]
         return dict(sorted(out.items()))
 
+    def _update_general(self, request, state, requirements) -> MaterialPointResponse:
+        """One general-mesh RVE solve per macro point from its committed state, in point order."""
+        from .rve import RVERequest, RVEState, build_rve_operator_cache, solve_rve_microequilibrium
+
+        if "general" not in self._batches:
+            self._batches["general"] = build_rve_operator_cache(self.model, linear_solver=self.linear_solver)
+        cache = self._batches["general"]
+        n = int(request.strains.shape[0])
+        host = not isinstance(request.strains, torch.Tensor)
+        variables = state.variables
+        copy = lambda v: v.clone() if isinstance(v, torch.Tensor) else np.array(v, copy=True)  # noqa: E731
+        nxt = {k: copy(v) for k, v in variables.items()}
+        stresses = np.zeros((n, 6))
+        tangents = np.zeros((n, 6, 6)) if requirements.tangent else None
+        psi = np.zeros(n) if requirements.free_energy else None
+        diss = np.zeros(n) if requirements.dissipation else None
+        rows = []
+        for i in range(n):
+            committed = RVEState(
+                MaterialState({k.removeprefix("rve_material__"): v[i] for k, v in variables.items()
+                               if k.startswith("rve_material__")}),
+                variables["rve_macro_strain"][i], variables["rve_fluctuation_dofs"][i])  # fmt: skip
+            resp = solve_rve_microequilibrium(self.model, RVERequest(request.strains[i], request.time_step,
+                                                                     request.update_settings, requirements),
+                                              committed, cache)  # fmt: skip
+            stresses[i] = _host(resp.macro_stress)
+            if tangents is not None:
+                tangents[i] = _host(resp.effective_tangent)
+            if psi is not None:
+                psi[i] = resp.free_energy_density
+            if diss is not None:
+                diss[i] = resp.dissipation_density
+            nxt["rve_macro_strain"][i] = _like(resp.state.macro_strain, nxt["rve_macro_strain"])
+            nxt["rve_fluctuation_dofs"][i] = _like(resp.state.fluctuation_dofs, nxt["rve_fluctuation_dofs"])
+            for k, v in resp.state.material_state.variables.items():
+                nxt[f"rve_material__{k}"][i] = _like(v, nxt[f"rve_material__{k}"])
+            rows.append(_general_macro_diagnostics(resp, self.model, cache))
+        names = sorted(set().union(*(r.keys() for r in rows)))
+        dev = None if host else request.strains.device
+        out = (lambda a: a) if host else (lambda a: None if a is None else torch.as_tensor(a, device=dev))  # noqa: E731
+        return MaterialPointResponse(
+            stresses=out(stresses), state=MaterialState(nxt), tangents=out(tangents), free_energy=out(psi),
+            dissipation=out(diss), diagnostics={k: out(np.asarray([r[k] for r in rows])) for k in names},
+        )  # fmt: skip
+
     def close(self) -> None:
         """Release the device batches."""
         self._batches.clear()
+
+
+def _host(value) -> np.ndarray:
+    return value.detach().cpu().numpy() if isinstance(value, torch.Tensor) else np.asarray(value)
+
+
+def _like(value, target):
+    """``value`` in the array type of ``target`` (host array or device tensor)."""
+    if isinstance(target, torch.Tensor):
+        return torch.as_tensor(_host(value), dtype=target.dtype, device=target.device)
+    return _host(value)
+
+
+def _general_macro_diagnostics(response, model, cache) -> dict[str, float]:
+    """The reference's reduction of one RVE response to macro-point values (material.py:218-264)."""
+    d = response.diagnostics
+    out = {
+        "incremental_work_density": float(d["positive_work_density"] + d["negative_work_density"]),
+        "viscoplastic_active": float(d["viscoplastic_active_volume_fraction"]),
+        "yield_activation_margin": float(d["minimum_yield_activation_margin"]),
+        "micro_newton_iterations": float(d["newton_iterations"]),
+        "micro_armijo_backtracks": float(d["armijo_backtracks"]),
+        "hill_mandel_error": float(d["hill_mandel_error"]),
+    }
+    weights = np.asarray(cache.quadrature_weights)
+    state = response.state.material_state.variables
+    if "equivalent_plastic_strain" in state:
+        out["equivalent_plastic_strain"] = float(np.sum(_host(state["equivalent_plastic_strain"]) * weights) / np.sum(weights))
+    stresses = _host(response.micro_stresses)
+    for phase_id, name in enumerate(model.phase_names):
+        mask = np.asarray(cache.point_phase_ids) == phase_id
+        pw = weights[mask]
+        out[f"phase_{name}__volume_fraction"] = float(np.sum(pw) / np.sum(weights))
+        phase_stress = np.sum(stresses[mask] * pw[:, None], axis=0) / np.sum(pw)
+        for comp, value in zip(_COMPONENTS, phase_stress):
+            out[f"phase_{name}__stress_{comp}"] = float(value)
+        key = f"phase_{name}__equivalent_plastic_strain"
+        if key in state:
+            q = _host(state[key])
+            out[key] = float(np.sum(q * pw) / np.sum(pw))
+            out[f"phase_{name}__maximum_equivalent_plastic_strain"] = float(np.max(q))
+    return out
 
 
 __all__ = ["RVEHomogenizedMaterial", "build_rve_operator_cache"]

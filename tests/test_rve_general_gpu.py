@@ -5,7 +5,9 @@
   tangent, fluctuation and displacement, Newton iterations, the consistency diagnostics;
 * the same path through solve_prescribed_rve_path (dispatch from the operator cache);
 * a structured box RVE solved by the general path against the batched box path (two
-  independent device implementations of the same solve).
+  independent device implementations of the same solve);
+* the FE2 macro adapter (RVEHomogenizedMaterial) with O-grid RVEs at its points against
+  single solves, with the reference's macro diagnostics.
 """
 
 from __future__ import annotations
@@ -17,7 +19,7 @@ pytestmark = pytest.mark.gpu
 
 from conftest import load_case  # noqa: E402
 from concrete_impact_b200.materials import (J2ViscoplasticMaterial, LinearElasticMaterial,  # noqa: E402
-                                            MaterialResponseRequirements, MaterialUpdateSettings)
+                                            MaterialPointRequest, MaterialResponseRequirements, MaterialUpdateSettings)
 from concrete_impact_b200.rve import (NonlinearNewtonSettings, RVERequest, build_rve_operator_cache,  # noqa: E402
                                       initialize_rve_state, solve_prescribed_rve_path, solve_rve_microequilibrium)
 from concrete_impact_b200.rve_builders import (build_cylindrical_ogrid_hex8, build_cylindrical_two_phase_rve,  # noqa: E402
@@ -99,3 +101,31 @@ def test_general_path_matches_box_path_on_a_box_rve() -> None:
         _close(gen.effective_tangent, np.asarray(box.effective_tangent), 1e-8, "effective_tangent")
         _close(gen.state.fluctuation_dofs, np.asarray(box.state.fluctuation_dofs), 1e-8, "fluctuation")
         assert abs(gen.diagnostics["newton_iterations"] - box.diagnostics["newton_iterations"]) <= 1
+
+
+def test_fe2_adapter_with_ogrid_rves_matches_single_solves() -> None:
+    from concrete_impact_b200.rve_material import RVEHomogenizedMaterial
+
+    g, meta = load_case("rve_ogrid_cylinder")
+    model = _ogrid_model(meta)
+    adapter = RVEHomogenizedMaterial(model, "ogrid_rve")
+    strains = np.stack([g[f"s{k}__macro_strain"] for k in range(3)])
+    request = MaterialPointRequest(strains, strains / meta["time_step"], meta["time_step"], "three_dimensional", UPDATE)
+    state = adapter.initialize_state(3)
+    resp = adapter.update(request, state, MaterialResponseRequirements(tangent=True, free_energy=True, dissipation=True))
+    cache = build_rve_operator_cache(model)
+    for i in range(3):
+        single = solve_rve_microequilibrium(model, RVERequest(strains[i], meta["time_step"], UPDATE,
+                                                              MaterialResponseRequirements(tangent=True)),
+                                            initialize_rve_state(model), cache)  # fmt: skip
+        np.testing.assert_allclose(resp.stresses[i], single.macro_stress, rtol=0, atol=1e-12 * np.abs(single.macro_stress).max())
+        np.testing.assert_allclose(resp.tangents[i], single.effective_tangent, rtol=0,
+                                   atol=1e-12 * np.abs(single.effective_tangent).max())  # fmt: skip
+        np.testing.assert_allclose(resp.state.variables["rve_fluctuation_dofs"][i], single.state.fluctuation_dofs,
+                                   rtol=0, atol=1e-12 * max(np.abs(single.state.fluctuation_dofs).max(), 1e-30))  # fmt: skip
+    assert np.all(state.variables["rve_macro_strain"] == 0.0)  # the committed state is untouched
+    np.testing.assert_array_equal(resp.state.variables["rve_macro_strain"], strains)
+    for key in ("incremental_work_density", "viscoplastic_active", "hill_mandel_error", "micro_newton_iterations",
+                "phase_matrix__volume_fraction", "phase_inclusion__stress_xx", "phase_matrix__equivalent_plastic_strain"):
+        assert resp.diagnostics[key].shape == (3,), key
+    assert resp.diagnostics["phase_matrix__equivalent_plastic_strain"][2] > 0.0
