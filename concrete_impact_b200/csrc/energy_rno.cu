@@ -112,7 +112,21 @@ __device__ float* forward_hidden(const NetView& n, int hidden, int layers, const
       const float bj = b[j];
 #pragma unroll
       for (int p = 0; p < ER_TILE; ++p) acc[p] = bj;
-      for (int k = 0; k < in_l; ++k) {
+      int k = 0;
+      for (; k + 4 <= in_l; k += 4) {  // four weights in flight per thread
+        const float w0 = Wt[(int64_t)k * hidden + j], w1 = Wt[(int64_t)(k + 1) * hidden + j];
+        const float w2 = Wt[(int64_t)(k + 2) * hidden + j], w3 = Wt[(int64_t)(k + 3) * hidden + j];
+#pragma unroll
+        for (int g = 0; g < ER_TILE / 4; ++g) {
+          const float4 v0 = *grp(hin, k, g), v1 = *grp(hin, k + 1, g), v2 = *grp(hin, k + 2, g),
+                       v3 = *grp(hin, k + 3, g);
+          acc[4 * g] = fmaf(w3, v3.x, fmaf(w2, v2.x, fmaf(w1, v1.x, fmaf(w0, v0.x, acc[4 * g]))));
+          acc[4 * g + 1] = fmaf(w3, v3.y, fmaf(w2, v2.y, fmaf(w1, v1.y, fmaf(w0, v0.y, acc[4 * g + 1]))));
+          acc[4 * g + 2] = fmaf(w3, v3.z, fmaf(w2, v2.z, fmaf(w1, v1.z, fmaf(w0, v0.z, acc[4 * g + 2]))));
+          acc[4 * g + 3] = fmaf(w3, v3.w, fmaf(w2, v2.w, fmaf(w1, v1.w, fmaf(w0, v0.w, acc[4 * g + 3]))));
+        }
+      }
+      for (; k < in_l; ++k) {
         const float w = Wt[(int64_t)k * hidden + j];
 #pragma unroll
         for (int g = 0; g < ER_TILE / 4; ++g) {
@@ -176,7 +190,20 @@ __device__ void input_gradient(const NetView& n, int hidden, int layers, const S
       float acc[ER_TILE];
 #pragma unroll
       for (int p = 0; p < ER_TILE; ++p) acc[p] = 0.0f;
-      for (int jj = 0; jj < hidden; ++jj) {
+      int jj = 0;
+      for (; jj + 4 <= hidden; jj += 4) {
+        const float w0 = W[(int64_t)jj * in_l + t], w1 = W[(int64_t)(jj + 1) * in_l + t];
+        const float w2 = W[(int64_t)(jj + 2) * in_l + t], w3 = W[(int64_t)(jj + 3) * in_l + t];
+#pragma unroll
+        for (int q = 0; q < ER_TILE / 4; ++q) {
+          const float4 v0 = *grp(d, jj, q), v1 = *grp(d, jj + 1, q), v2 = *grp(d, jj + 2, q), v3 = *grp(d, jj + 3, q);
+          acc[4 * q] = fmaf(v3.x, w3, fmaf(v2.x, w2, fmaf(v1.x, w1, fmaf(v0.x, w0, acc[4 * q]))));
+          acc[4 * q + 1] = fmaf(v3.y, w3, fmaf(v2.y, w2, fmaf(v1.y, w1, fmaf(v0.y, w0, acc[4 * q + 1]))));
+          acc[4 * q + 2] = fmaf(v3.z, w3, fmaf(v2.z, w2, fmaf(v1.z, w1, fmaf(v0.z, w0, acc[4 * q + 2]))));
+          acc[4 * q + 3] = fmaf(v3.w, w3, fmaf(v2.w, w2, fmaf(v1.w, w1, fmaf(v0.w, w0, acc[4 * q + 3]))));
+        }
+      }
+      for (; jj < hidden; ++jj) {
         const float w = W[(int64_t)jj * in_l + t];
 #pragma unroll
         for (int q = 0; q < ER_TILE / 4; ++q) {
