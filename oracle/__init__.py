@@ -12,7 +12,14 @@ never imports it.
                           reference's CPU cost where the reference itself cannot run).
 * ``oracle/j2vp_oracle.c`` -- plain-C restatement of the batched incremental form,
                           multi-threaded with OpenMP, used as the strong CPU baseline.
-* ``oracle.rve``        -- NumPy/SciPy restatement of the periodic Hex8 RVE Newton solve.
+* ``oracle.rve``        -- NumPy/SciPy restatement of the periodic Hex8 RVE Newton solve;
+  ``oracle.rve_general`` -- the same on any mesh with topology-provided periodic classes.
+* ``oracle.fe2``        -- explicit macro dynamics of a linear elastic bar.
+* ``oracle.newmark``    -- implicit Newmark material dynamics (the reference's
+                          solve_material_implicit_newmark) with J2 points or RVE solves.
+* ``oracle.rno`` / ``oracle.rno_torch`` -- the package's recurrent surrogate window and a
+                          host torch training loop (CPU baseline).
+* ``oracle.rno_energy`` -- the reference's energy-based RVE-RNO update.
 
 Parity pin: every function is checked against golden vectors produced by running the
 reference implementation itself (``tests/golden/make_golden.py``) and against the
