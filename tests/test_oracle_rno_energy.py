@@ -81,3 +81,24 @@ def test_packed_parameters_follow_the_kernel_layout() -> None:
         pack_state_dict(cfg, dict(sd, extra=np.zeros(1)))
     with pytest.raises(ValueError):
         RVERNOModelConfig(**dict({k: v for k, v in meta["model"].items() if k != "device"}, strain_input_scale=(1.0,)))
+
+
+def test_loader_rejects_mismatched_artifact_metadata(tmp_path) -> None:
+    """The architecture contract is checked before any device work (deployment.py:36-57)."""
+    import json
+
+    from concrete_impact_b200.energy_rno import load_rve_rno_state_dict
+
+    _, meta, _ = _case()
+    spec = {k: v for k, v in meta["model"].items() if k != "device"}
+    metadata = {"model_family": spec["family"], "deployment_integrator": "explicit_only",
+                **{k: spec[k] for k in ("integrator", "evolution", "reference_time_scale", "latent_dimension",
+                                        "hidden_size", "hidden_layers", "activation", "dtype")}}  # fmt: skip
+    metadata["hidden_size"] = 64
+    (tmp_path / "meta.json").write_text(json.dumps(metadata))
+    with pytest.raises(ValueError, match="does not match"):
+        load_rve_rno_state_dict(RVERNOModelConfig(**spec), tmp_path / "missing.pt", tmp_path / "meta.json")
+    with pytest.raises(ValueError):
+        RVERNOModelConfig(**dict(spec, integrator="backward_euler"))
+    with pytest.raises(ValueError):
+        RVERNOModelConfig(**dict(spec, reference_time_scale=0.0))
