@@ -113,3 +113,26 @@ def test_step_control_rules_and_armijo_search() -> None:
     assert (res.step_length, res.backtracks) == (0.5, 1)
     with pytest.raises(ArmijoLineSearchError):
         perform_armijo_search(1.0, lambda step: 2.0, ArmijoSettings(enabled=True, max_backtracks=3))
+
+
+def test_average_acceleration_conserves_energy_on_an_elastic_bar() -> None:
+    """Newmark with beta = 1/4, gamma = 1/2 conserves the discrete energy of a linear
+    system: with the J2 yield stress out of reach the oracle's energy residual (kinetic +
+    free + dissipated - external work) stays at roundoff over a pulse and its free
+    vibration."""
+    nodes, elements = box_mesh((0.06, 0.01, 0.01), (6, 1, 1))
+    elastic = oj.J2Params(25.0e9, 0.2, 1.0e12, 2.0e9, 1.0e-3, 1.0e12, 1.0)
+    bar = on.Bar(nodes, elements, 2200.0)
+    fixed = (3 * np.flatnonzero(np.isclose(nodes[:, 0], 0.0))[:, None] + np.arange(3)).ravel()
+    unit = np.zeros(3 * nodes.shape[0])
+    unit[3 * np.flatnonzero(np.isclose(nodes[:, 0], 0.06))] = -1.0e-4 / 4.0
+
+    def load(t):
+        return (5.0e6 * math.sin(math.pi * t / 10.0e-6) if t <= 10.0e-6 else 0.0) * unit
+
+    newton = dict(max_iterations=10, residual_absolute_tolerance=1e-9, residual_relative_tolerance=1e-12,
+                  increment_absolute_tolerance=1e-16, increment_relative_tolerance=1e-12, armijo=None)  # fmt: skip
+    out = on.implicit_newmark(bar, on.PointJ2(elastic), fixed, load, 2.0e-6, 30, 0.25, 0.5, newton)
+    assert np.all(out["dissipated_energy"] == 0.0)
+    assert np.abs(out["energy_residual"]).max() <= 1e-9 * out["external_work"].max()
+    assert out["kinetic_energy"][-1] > 0.0  # still vibrating after the pulse

@@ -85,3 +85,24 @@ def test_general_oracle_matches_reference_ogrid_rve() -> None:
             np.testing.assert_allclose(out[key], ref, rtol=0, atol=1e-13 * np.abs(ref).max(), err_msg=key)
         np.testing.assert_allclose(state["w"], g[f"s{step}__fluctuation"], rtol=0,
                                    atol=1e-12 * np.abs(g[f"s{step}__fluctuation"]).max())  # fmt: skip
+
+
+@pytest.mark.parametrize("divisions", [(8, 2, 2), (16, 4, 3), (32, 8, 2)])
+def test_ogrid_meshes_are_valid_periodic_cells(divisions) -> None:
+    """Positive Jacobians, the cell volume, an inclusion area converging to the target
+    fraction, and periodic classes that pair every boundary node with its images."""
+    from oracle.rve import b_matrices
+
+    c, r, a = divisions
+    mesh = build_cylindrical_ogrid_hex8((1.0, 0.8, 0.5), 0.3, c, r, a)
+    _, det = b_matrices(mesh.nodes, mesh.elements)
+    assert det.min() > 0.0
+    assert det.sum() == pytest.approx(1.0 * 0.8 * 0.5, rel=1e-12)
+    # the inscribed polygon of c sides misses O(1/c^2) of the circle's area
+    assert 0.0 < 1.0 - mesh.discrete_inclusion_area / (0.3 * 0.8) < {8: 0.1, 16: 0.04, 32: 0.01}[c]
+    cls = mesh.periodic_class_ids
+    for (minus, plus), axis in zip(mesh.opposite_face_nodes, range(3)):
+        np.testing.assert_array_equal(cls[minus], cls[plus])
+        shift = mesh.nodes[plus] - mesh.nodes[minus]
+        np.testing.assert_allclose(shift[:, axis], (1.0, 0.8, 0.5)[axis], rtol=1e-12)
+        np.testing.assert_allclose(np.delete(shift, axis, axis=1), 0.0, atol=1e-12)
