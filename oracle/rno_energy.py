@@ -92,3 +92,21 @@ def update(sd: dict, strain, latent, time_step, reference_time_scale: float, int
             "dimensionless_state_rate": rate_dimless, "dissipation": dissipation,
             "free_energy": equilibrium + resp_neq, "thermodynamic_violation": np.maximum(-dissipation, 0.0),
             "nonequilibrium_energy_increment": cand_neq - prev_neq}  # fmt: skip
+
+
+def tangent_fd(sd: dict, strain, latent, time_step, reference_time_scale: float, integrator: str,
+               strain_scale=None, anchor: dict | None = None, relative_step: float = 1.0e-6) -> np.ndarray:
+    """d stress / d strain (B, 6, 6) by central differences of ``update`` in float64 -- the
+    quantity the reference obtains by automatic differentiation (rve_rno.py:280-293), with
+    the candidate latent state following the strain through the forward-Euler step."""
+    strain = np.asarray(strain, dtype=np.float64)
+    a = anchor or anchors(sd, np.asarray(latent).shape[1])
+    h = relative_step * max(float(np.abs(strain).max()), 1.0e-3)
+    out = np.zeros((strain.shape[0], 6, 6))
+    for c in range(6):
+        e = np.zeros(6)
+        e[c] = h
+        plus = update(sd, strain + e, latent, time_step, reference_time_scale, integrator, strain_scale, a)["stress"]
+        minus = update(sd, strain - e, latent, time_step, reference_time_scale, integrator, strain_scale, a)["stress"]
+        out[:, :, c] = (plus - minus) / (2.0 * h)
+    return out

@@ -470,6 +470,9 @@ def make_rno_energy_cases(src: str):
                 other = models["cs_semi_implicit_forward_euler"].update_batch(strain, latent, time_step, anchors)
                 for k in keys:
                     semi[k].append(getattr(other, k).numpy())
+                with torch.enable_grad():  # the algorithmic tangent (autograd) of 16 points
+                    tan = main.update_batch(strain[:16], latent[:16], time_step[:16], anchors, compute_tangent=True)
+                    arrays["tangent_last16"] = tan.tangent.detach().numpy()
             latent = res.latent_state
     arrays.update(strain=np.stack(strains), latent_in=np.stack(latents_in), time_step=dt.astype(np.float32))
     arrays.update({f"out__{k}": np.stack(v) for k, v in out.items()})

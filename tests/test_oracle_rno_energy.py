@@ -102,3 +102,14 @@ def test_loader_rejects_mismatched_artifact_metadata(tmp_path) -> None:
         RVERNOModelConfig(**dict(spec, integrator="backward_euler"))
     with pytest.raises(ValueError):
         RVERNOModelConfig(**dict(spec, reference_time_scale=0.0))
+
+
+def test_oracle_tangent_matches_reference_autograd_tangent() -> None:
+    """Central differences of the float64 update against the reference's FP32 autograd
+    tangent of 16 points at the last rollout step (the GPU path does not provide it yet)."""
+    g, meta, sd = _case()
+    last = meta["steps"] - 1
+    ref = g["tangent_last16"]
+    tan = oe.tangent_fd(sd, g["strain"][last][:16], g["latent_in"][last][:16], g["time_step"][:16],
+                        meta["model"]["reference_time_scale"], meta["model"]["integrator"])  # fmt: skip
+    np.testing.assert_allclose(tan, ref, rtol=0, atol=1e-4 * np.abs(ref).max())
