@@ -15,7 +15,7 @@ KEYS = {"impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_
         "dtype", "data", "config", "cpu_baseline", "e2e"}
 
 
-@pytest.mark.parametrize("workload", ["return_map", "rve_path", "rno_train", "implicit_fe2"])
+@pytest.mark.parametrize("workload", ["return_map", "rve_path", "rno_train", "implicit_fe2", "rno_energy"])
 def test_reference_arm_prints_one_contract_line(workload: str) -> None:
     cmd = [sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--workload", workload, "--steps", "1",
            "--warmup", "1"]
