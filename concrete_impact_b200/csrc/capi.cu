@@ -1,6 +1,9 @@
 // Library-wide C entry points: names, reasons, version and error reporting.
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <vector>
+
 #include "cib_common.cuh"
 
 namespace cib {
@@ -20,6 +23,32 @@ int sm_count() {
     cached[dev] = n;
   }
   return cached[dev];
+}
+
+int allow_dynamic_smem(const void* kernel, int bytes) {
+  struct Entry {
+    const void* kernel;
+    int dev;
+    int bytes;
+  };
+  static std::mutex mutex;
+  static std::vector<Entry> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    last_cuda_error_slot() = (int)e;
+    return CIB_ECUDA;
+  }
+  std::lock_guard<std::mutex> lock(mutex);
+  for (const Entry& x : done)
+    if (x.kernel == kernel && x.dev == dev && x.bytes >= bytes) return CIB_OK;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) {
+    last_cuda_error_slot() = (int)e;
+    return CIB_ECUDA;
+  }
+  done.push_back({kernel, dev, bytes});
+  return CIB_OK;
 }
 
 }  // namespace cib

@@ -26,6 +26,11 @@ inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Raise a kernel's dynamic shared-memory limit to `bytes` on the current device.  The
+// attribute is per device, so the call is made (and remembered) once per kernel and device;
+// returns CIB_OK or CIB_ECUDA (with the CUDA error recorded).
+int allow_dynamic_smem(const void* kernel, int bytes);
+
 // Grid for a grid-stride kernel: whole waves of resident blocks (SMs x blocks per SM),
 // capped by the work available.
 inline int persistent_grid(const void* kernel, int threads, int64_t work_items, size_t smem = 0) {

@@ -377,13 +377,8 @@ inline size_t energy_smem(int hidden, int layers) {
 int launch_energy(const cib_energy_rno* m, const EnergyArgs& a, int64_t blocks, cudaStream_t st) {
   const size_t smem = energy_smem(m->hidden, m->layers);
   if (smem > 200 * 1024) return CIB_ERANGE;
-  static bool configured = false;
-  if (!configured) {
-    if (cudaFuncSetAttribute(energy_rno_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
-        cudaSuccess)
-      return check_launch();
-    configured = true;
-  }
+  const int rc = allow_dynamic_smem(reinterpret_cast<const void*>(energy_rno_kernel), 200 * 1024);
+  if (rc != CIB_OK) return rc;
   energy_rno_kernel<<<(unsigned)blocks, ER_THREADS, smem, st>>>(a);
   return check_launch();
 }

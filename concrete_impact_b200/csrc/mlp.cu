@@ -257,7 +257,8 @@ extern "C" int cib_mlp_gemm(int32_t epilogue, int32_t M, int32_t N, int32_t K, c
 extern "C" int cib_splitk_reduce(int32_t M, int32_t N, int32_t splits, const float* partial, int32_t ldc, float* out,
                                  int32_t ldo, void* stream) {
   if (M < 0 || N < 0 || splits < 1 || !partial || !out) return CIB_EINVAL;
-  if (M * N == 0) return CIB_OK;
+  if ((int64_t)M * N > (int64_t)INT32_MAX - 256) return CIB_ERANGE;  // 32-bit element index
+  if ((int64_t)M * N == 0) return CIB_OK;
   const int threads = 256;
   splitk_reduce_kernel<<<(M * N + threads - 1) / threads, threads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       M, N, splits, partial, ldc, out, ldo);

@@ -133,6 +133,10 @@ __global__ void counter_increment_kernel(int* counter) {
 
 inline unsigned nblk(int n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// The elementwise kernels index with 32-bit ints: sizes whose element count (rows x
+// components) would not fit are refused with CIB_ERANGE before anything is launched.
+inline bool fits_int32(int64_t a, int64_t b) { return a * b <= (int64_t)INT32_MAX - 256; }
+
 }  // namespace
 }  // namespace cib
 
@@ -141,6 +145,7 @@ using namespace cib;
 extern "C" int cib_rno_input(int32_t B, const float* strain, const float* rate, const float* z, void* X, void* Xt,
                              int32_t ldxt, int32_t row_offset, void* stream) {
   if (B < 0 || !strain || !rate || !z || !X) return CIB_EINVAL;
+  if (!fits_int32(B, RNO_IN)) return CIB_ERANGE;
   if (B == 0) return CIB_OK;
   rno_input_kernel<<<nblk(B * RNO_IN, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       B, strain, rate, z, static_cast<__nv_bfloat16*>(X), static_cast<__nv_bfloat16*>(Xt), ldxt, row_offset);
@@ -150,6 +155,7 @@ extern "C" int cib_rno_input(int32_t B, const float* strain, const float* rate, 
 extern "C" int cib_rno_forward_tail(int32_t B, const float* Y, const float* target, const float* coef, const float* z,
                                     float* z_next, float* gY, float loss_scale, double* loss_part, void* stream) {
   if (B < 0 || !Y || !coef || !z || !z_next) return CIB_EINVAL;
+  if (!fits_int32(B, RNO_OUT)) return CIB_ERANGE;
   if (B == 0) return CIB_OK;
   rno_forward_tail_kernel<<<nblk(B, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       B, Y, target, coef, z, z_next, gY, loss_scale, loss_part);
@@ -159,6 +165,7 @@ extern "C" int cib_rno_forward_tail(int32_t B, const float* Y, const float* targ
 extern "C" int cib_rno_backward_head(int32_t B, const float* gY, const float* coef, const float* dz_next, void* dY,
                                      void* dYt, int32_t lddyt, int32_t row_offset, void* stream) {
   if (B < 0 || !gY || !coef || !dz_next || !dY) return CIB_EINVAL;
+  if (!fits_int32(B, RNO_OUT)) return CIB_ERANGE;
   if (B == 0) return CIB_OK;
   rno_backward_head_kernel<<<nblk(B * RNO_OUT, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       B, gY, coef, dz_next, static_cast<__nv_bfloat16*>(dY), static_cast<__nv_bfloat16*>(dYt), lddyt, row_offset);
@@ -167,6 +174,7 @@ extern "C" int cib_rno_backward_head(int32_t B, const float* gY, const float* co
 
 extern "C" int cib_rno_backward_tail(int32_t B, const float* dz_next, const float* dX, float* dz, void* stream) {
   if (B < 0 || !dz_next || !dX || !dz) return CIB_EINVAL;
+  if (!fits_int32(B, RNO_IN)) return CIB_ERANGE;
   if (B == 0) return CIB_OK;
   rno_backward_tail_kernel<<<nblk(B * 6, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(B, dz_next, dX, dz);
   return check_launch();
@@ -184,7 +192,8 @@ extern "C" int cib_adam_step(int32_t rows, int32_t cols, float* w, const float* 
                              float beta1, float beta2, float eps, const int32_t* step, void* Wb, int32_t ldb, void* Wt,
                              int32_t ldt, void* stream) {
   if (rows < 0 || cols < 0 || !w || !g || !m || !v || !step) return CIB_EINVAL;
-  if (rows * cols == 0) return CIB_OK;
+  if (!fits_int32(rows, cols)) return CIB_ERANGE;
+  if ((int64_t)rows * cols == 0) return CIB_OK;
   adam_kernel<<<nblk(rows * cols, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
       rows, cols, w, g, m, v, lr, beta1, beta2, eps, step, static_cast<__nv_bfloat16*>(Wb), ldb,
       static_cast<__nv_bfloat16*>(Wt), ldt);

@@ -411,16 +411,6 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
 
 // The dynamic shared-memory limit is raised once per device and kernel (so that launches
 // recorded into a CUDA graph make no attribute call).
-bool prepare_attributes(const void* fn, size_t bytes, int which) {
-  static bool done[2][64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
-  if (done[which][dev]) return true;
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return false;
-  done[which][dev] = true;
-  return true;
-}
-
 int validate_common(const cib_rno_window* w) {
   if (!w || w->B < 0 || w->T < 1 || w->hidden != HID || !w->strain || !w->rate || !w->coef || !w->z || !w->err)
     return CIB_EINVAL;
@@ -442,7 +432,8 @@ extern "C" int cib_rno_window_forward(const cib_rno_window* w, void* stream) {
   if (w->gS && !w->target) return CIB_EINVAL;
   if (w->B == 0) return CIB_OK;
   const size_t bytes = sizeof(FwdSmem);
-  if (!prepare_attributes(reinterpret_cast<const void*>(rno_window_forward_kernel), bytes, 0)) return CIB_ECUDA;
+  if (allow_dynamic_smem(reinterpret_cast<const void*>(rno_window_forward_kernel), (int)bytes) != CIB_OK)
+    return CIB_ECUDA;
   const unsigned grid = (unsigned)((w->B + TILE - 1) / TILE);
   rno_window_forward_kernel<<<grid, RW_THREADS, bytes, reinterpret_cast<cudaStream_t>(stream)>>>(*w);
   return check_launch();
@@ -457,7 +448,8 @@ extern "C" int cib_rno_window_backward(const cib_rno_window* w, void* stream) {
   if (!w->gS || !w->dYt) return CIB_EINVAL;
   if (w->B == 0) return CIB_OK;
   const size_t bytes = sizeof(BwdSmem);
-  if (!prepare_attributes(reinterpret_cast<const void*>(rno_window_backward_kernel), bytes, 1)) return CIB_ECUDA;
+  if (allow_dynamic_smem(reinterpret_cast<const void*>(rno_window_backward_kernel), (int)bytes) != CIB_OK)
+    return CIB_ECUDA;
   const unsigned grid = (unsigned)((w->B + TILE - 1) / TILE);
   rno_window_backward_kernel<<<grid, RW_THREADS, bytes, reinterpret_cast<cudaStream_t>(stream)>>>(*w);
   return check_launch();

@@ -567,6 +567,15 @@ __global__ void __launch_bounds__(RVE_THREADS, 2) rve_pcg_kernel(const RvePcgArg
   const RveDesc d = a.desc[r];
   const int64_t E = (int64_t)d.nx * d.ny * d.nz;
   const int64_t off = a.sys_off[s];  // vector offset of this system (3 * node base)
+  if (a.vec_len >= 0 && (off < 0 || E < 0 || off + 3 * E > a.vec_len)) {  // uniform over the CTA
+    if (threadIdx.x == 0) {
+      a.status[s] = 3;
+      a.iterations[s] = 0;
+      a.rel_residual[s] = 0.0;
+      a.xnorm[s] = 0.0;
+    }
+    return;
+  }
   const double* b = a.b + off;
   double* x = a.x + off;
   double* rr = a.r + off;
@@ -1288,14 +1297,8 @@ template <typename T>
 int launch_rve_pcg(const RvePcgArgs<T>& a, int nsys, int max_nxy, cudaStream_t st) {
   const size_t smem = (size_t)max_nxy * (24 + 9) * sizeof(double);
   if (smem > 200 * 1024) return CIB_ERANGE;
-  static bool configured[2] = {false, false};
-  const int slot = sizeof(T) == 8 ? 1 : 0;
-  if (!configured[slot]) {
-    if (cudaFuncSetAttribute(rve_pcg_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
-        cudaSuccess)
-      return check_launch();
-    configured[slot] = true;
-  }
+  const int rc = allow_dynamic_smem(reinterpret_cast<const void*>(rve_pcg_kernel<T>), 200 * 1024);
+  if (rc != CIB_OK) return rc;
   rve_pcg_kernel<T><<<nsys, RVE_THREADS, smem, st>>>(a);
   return check_launch();
 }
@@ -1306,14 +1309,8 @@ int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cl
   if (cluster != 2 && cluster != 4 && cluster != 8) return CIB_EINVAL;
   const size_t smem = (size_t)max_nxy * (24 * sizeof(T) + 12 * sizeof(double));
   if (smem > 200 * 1024) return CIB_ERANGE;
-  static bool configured[2] = {false, false};
-  const int slot = sizeof(T) == 8 ? 1 : 0;
-  if (!configured[slot]) {
-    if (cudaFuncSetAttribute(rve_pcg_cluster_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
-        cudaSuccess)
-      return check_launch();
-    configured[slot] = true;
-  }
+  const int rc = allow_dynamic_smem(reinterpret_cast<const void*>(rve_pcg_cluster_kernel<T>), 200 * 1024);
+  if (rc != CIB_OK) return rc;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)nsys * (unsigned)cluster, 1, 1);
   cfg.blockDim = dim3(RVE_THREADS, 1, 1);

@@ -118,6 +118,10 @@ struct RvePcgArgs {
   int32_t* iterations;
   double* rel_residual;
   double* xnorm;
+  // Length of the vectors r, p, Ap when they belong to the library (no-allocation entry):
+  // a system whose entries would leave [0, vec_len) is skipped with status 3.  -1: the
+  // caller owns the vectors and sizes them (not checked).
+  int64_t vec_len = -1;
 };
 
 template <typename T>

@@ -28,10 +28,46 @@ namespace cib {
 namespace {
 
 // Device address of g_pcg_work per device.  In host code the name g_pcg_work is only a
-// host-side stand-in for the device symbol, so the real address is looked up once per
-// device with that device current.
+// host-side stand-in for the device symbol, so the real address is looked up with that
+// device current.  The lookup is remembered together with the CUDA context it was made in
+// (its unique context id): after cudaDeviceReset the device gets a new primary context, in
+// which the library's module -- and the array -- may sit elsewhere, so a changed id makes
+// the next call look the address up again (as does a driver without context ids, on every
+// call).
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+
+struct WorkSlot {
+  unsigned long long ctx_id;
+  double* ptr;
+};
+
 std::mutex g_work_mutex;
-double* g_work_ptr[64] = {nullptr};
+WorkSlot g_work_slot[64] = {};
+
+// Id of the calling thread's current context (0 when the driver entry points are missing).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    resolved = true;
+  }
+  if (!get_current || !get_id) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || ctx == nullptr || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 int work_address(double** out) {
   int dev = 0;
@@ -42,16 +78,19 @@ int work_address(double** out) {
   }
   if (dev < 0 || dev >= 64) return CIB_ERANGE;
   std::lock_guard<std::mutex> lock(g_work_mutex);
-  if (g_work_ptr[dev] == nullptr) {
+  const unsigned long long ctx = current_context_id();
+  WorkSlot& slot = g_work_slot[dev];
+  if (slot.ptr == nullptr || ctx == 0 || slot.ctx_id != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_pcg_work);
     if (e != cudaSuccess || p == nullptr) {
       last_cuda_error_slot() = (int)(e != cudaSuccess ? e : cudaErrorInvalidSymbol);
       return CIB_ECUDA;
     }
-    g_work_ptr[dev] = static_cast<double*>(p);
+    slot.ptr = static_cast<double*>(p);
+    slot.ctx_id = current_context_id();
   }
-  *out = g_work_ptr[dev];
+  *out = slot.ptr;
   return CIB_OK;
 }
 
@@ -105,6 +144,7 @@ int solve(const cib_rve_batch& b, int32_t nsys, const int32_t* sys_rve, const in
   a.iterations = iterations;
   a.rel_residual = rel;
   a.xnorm = xnorm;
+  a.vec_len = vec_len;  // a system outside the work array is skipped with status 3
   return launch_rve_pcg<T>(a, nsys, b.max_nxy, st);
 }
 
@@ -117,7 +157,7 @@ extern "C" int cib_rve_pcg_noalloc(const cib_rve_batch* batch, int32_t nsys, con
                                    const int64_t* sys_off, const int32_t* active, int64_t vec_len, const double* b,
                                    const double* dinv, double* x, double rtol, int32_t maxit, int32_t* status,
                                    int32_t* iterations, double* rel_residual, double* xnorm, void* stream) {
-  if (!batch || batch->nrve < 0 || batch->nphase < 1 || batch->nphase > RVE_MAX_PHASES || !batch->desc ||
+  if (!batch || batch->nrve < 0 || batch->nelem < 0 || batch->nphase < 1 || batch->nphase > RVE_MAX_PHASES || !batch->desc ||
       !batch->phase || (batch->precision != 32 && batch->precision != 64) || nsys < 0 || !sys_rve || !sys_off ||
       !b || !dinv || !x || !status || !iterations || !rel_residual || !xnorm || maxit < 0 || !batch->tparam ||
       !batch->tflag || batch->max_nxy <= 0 || vec_len < 0)

@@ -305,11 +305,14 @@ int cib_rve_pcg_cluster(const cib_rve_batch* batch, int32_t nsys, const int32_t*
  * 3 x CIB_PCG_NOALLOC_MAX_VEC doubles (1.5 MiB), held by every GPU that loads the library
  * until the process exits; nothing is allocated by the call.  vec_len is the length of b
  * and x (doubles) and every system's vectors must lie inside it, as for cib_rve_pcg;
- * vec_len > CIB_PCG_NOALLOC_MAX_VEC returns CIB_ERANGE without launching.  The first call
+ * vec_len > CIB_PCG_NOALLOC_MAX_VEC returns CIB_ERANGE without launching, and a system
+ * whose vectors (sys_off .. sys_off + 3 E) would leave [0, vec_len) is skipped on the
+ * device with status 3, so a wrong offset never writes outside the array.  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress) and should come
- * before any stream capture.  All calls on a device share the array: calls that overlap
- * on the GPU race and must not be issued; no content is carried from one call to the next.
- * Outputs and status codes are those of cib_rve_pcg. */
+ * before any stream capture; the address is looked up again when the device's context has
+ * changed (after cudaDeviceReset).  All calls on a device share the array: calls that
+ * overlap on the GPU race and must not be issued; no content is carried from one call to
+ * the next.  Outputs and other status codes are those of cib_rve_pcg. */
 #define CIB_PCG_NOALLOC_MAX_VEC 65536
 int cib_rve_pcg_noalloc(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve, const int64_t* sys_off,
                         const int32_t* active, int64_t vec_len, const double* b, const double* dinv, double* x,

@@ -1,8 +1,9 @@
 """Generate golden vectors by running the reference implementation itself.
 
-Run in a container that holds the reference checkout (read-only) at REFERENCE_SRC:
+Run in a container that holds the reference checkout (read-only); pass its ``src``
+directory, or set the environment variable CIB_REFERENCE_SRC:
 
-    python tests/golden/make_golden.py [--reference /root/reference/src]
+    python tests/golden/make_golden.py --reference <checkout>/src
 
 The reference imports gmsh, meshio and h5py at module level in files that the material
 and RVE paths never execute; empty stand-in modules are put on sys.path for them.  The
@@ -14,6 +15,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -487,10 +489,13 @@ GROUPS = ("j2", "rve", "newmark", "ogrid", "rno_energy")
 
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
-    parser.add_argument("--reference", default="/root/reference/src")
+    parser.add_argument("--reference", default=os.environ.get("CIB_REFERENCE_SRC"),
+                        help="the reference checkout's src directory (default: $CIB_REFERENCE_SRC)")
     parser.add_argument("--only", choices=GROUPS, action="append",
                         help="regenerate only these groups (default: all); the manifest keeps the other entries")
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("give --reference <checkout>/src or set CIB_REFERENCE_SRC")
     groups = set(args.only or GROUPS)
     _import_reference(args.reference)
     from fem.materials import data as data_mod

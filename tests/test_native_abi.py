@@ -139,3 +139,17 @@ def test_struct_layouts_match_c_header(tmp_path) -> None:
         assert int(got[name]) == ctypes.sizeof(cls), name
         for f in fields:
             assert int(got[f"{name}.{f}"]) == getattr(cls, f).offset, f"{name}.{f}"
+
+
+def test_sizes_beyond_32_bit_indexing_are_refused_without_a_launch() -> None:
+    """The surrogate's elementwise entry points index with 32-bit ints; batches whose
+    element count would overflow come back as CIB_ERANGE (-3) before any CUDA call."""
+    lib = _native.load_library()
+    big = 2**31 // 16  # B * 32 inputs per row overflows int32
+    fake = 256  # never dereferenced: the size check comes first
+    assert lib.cib_rno_input(big, fake, fake, fake, fake, None, 0, 0, None) == -3
+    assert lib.cib_rno_backward_tail(big, fake, fake, fake, None) == -3
+    assert lib.cib_rno_forward_tail(2**31 // 8, fake, None, fake, fake, fake, None, 1.0, None, None) == -3
+    assert lib.cib_adam_step(65536, 65536, fake, fake, fake, fake, 1e-3, 0.9, 0.999, 1e-8, fake, None, 0, None, 0,
+                             None) == -3  # fmt: skip
+    assert lib.cib_splitk_reduce(65536, 65536, 1, fake, 65536, fake, 65536, None) == -3

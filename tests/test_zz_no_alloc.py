@@ -91,3 +91,31 @@ def test_noalloc_pcg_rejects_sizes_beyond_its_work_array() -> None:
     )  # fmt: skip
     assert code == -3  # CIB_ERANGE: nothing launched
     assert torch.all(st == -7)
+
+
+def test_noalloc_pcg_skips_a_system_whose_offset_leaves_the_work_array() -> None:
+    """A system offset that would put r, p, Ap past vec_len is refused by the kernel's own
+    bounds check (status 3, nothing written); the other system is solved as usual."""
+    batch = _prepared_batch()
+    lib = _native.load_library()
+    b = batch.batch_struct(batch._settings_used)
+    vec_len = 3 * batch.nelem
+    x_ref, st_ref, it_ref, rel_ref, xn_ref = _outputs(batch)
+    batch.pcg(b, batch.res, x_ref, batch.r, batch.p, batch.Ap, batch.nrve, batch.sys_rve, batch.sys_off, st_ref,
+              it_ref, rel_ref, xn_ref)  # fmt: skip
+    bad_off = batch.sys_off.clone()
+    bad_off[1] = vec_len - 3  # the second RVE's 3 E entries would run past the end
+    x, st, it, rel, xn = _outputs(batch)
+    code = lib.cib_rve_pcg_noalloc(
+        ctypes.byref(b), batch.nrve, batch.sys_rve.data_ptr(), bad_off.data_ptr(), batch.active.data_ptr(),
+        vec_len, batch.res.data_ptr(), batch.dinv.data_ptr(), x.data_ptr(), float(batch.rtol),
+        int(batch.linear.max_iterations), st.data_ptr(), it.data_ptr(), rel.data_ptr(), xn.data_ptr(),
+        _native.stream_ptr(),
+    )  # fmt: skip
+    assert code == 0
+    torch.cuda.synchronize()
+    assert st.cpu().tolist() == [0, 3] and int(it[1]) == 0
+    n0 = 3 * int(batch.elem_counts[0])
+    np.testing.assert_allclose(x[:n0].cpu().numpy(), x_ref[:n0].cpu().numpy(), rtol=1e-12,
+                               atol=1e-12 * float(x_ref.abs().max()))  # fmt: skip
+    assert torch.isnan(x[n0:]).all()  # the skipped system's solution was never written
