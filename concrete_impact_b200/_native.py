@@ -129,6 +129,25 @@ class RVEBatchC(ctypes.Structure):
     ]
 
 
+class RVENewtonC(ctypes.Structure):
+    """``cib_rve_newton``: settings and device buffers of the device-controlled Newton solve."""
+
+    _fields_ = [
+        ("max_iterations", ctypes.c_int32),
+        ("inexact", ctypes.c_int32),
+        ("residual_absolute_tolerance", ctypes.c_double),
+        ("residual_relative_tolerance", ctypes.c_double),
+        ("increment_absolute_tolerance", ctypes.c_double),
+        ("increment_relative_tolerance", ctypes.c_double),
+        ("pcg_rtol", ctypes.c_double),
+        ("pcg_maxit", ctypes.c_int32),
+        ("cluster", ctypes.c_int32),
+    ] + [(name, ctypes.c_void_p) for name in (
+        "time_step", "macro", "w_n", "w", "w_out", "x", "r", "p", "Ap", "residual", "dinv", "rnorm2", "wnorm2",
+        "class_max", "alpha", "active", "live_mask", "fail", "sys_rve", "sys_off", "pcg_status", "pcg_iterations",
+        "pcg_rel_residual", "pcg_xnorm", "iwork", "dwork")]  # fmt: skip
+
+
 class RNOWindowC(ctypes.Structure):
     """``cib_rno_window``."""
 
@@ -226,6 +245,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_rve_tangent_rhs": (_I, [_P] * 6),
     "cib_rve_tangent_finish": (_I, [_P] * 7),
     "cib_rve_response": (_I, [_P] * 11),
+    "cib_rve_newton_workspace": (None, [ctypes.c_int32, _P, _P]),
+    "cib_rve_newton_graph_create": (_I, [_P, _P, _P]),
+    "cib_rve_newton_graph_launch": (_I, [_P, _P]),
+    "cib_rve_newton_graph_destroy": (_I, [_P]),
     "cib_j2_diagnostic_name": (ctypes.c_char_p, [_I]),
     "cib_j2_reason": (ctypes.c_char_p, [_I]),
     "cib_last_cuda_error": (_I, []),

@@ -258,28 +258,30 @@ __device__ __forceinline__ void load_w(const double* w, const double* dw, double
 
 // ---------------------------------------------------------------------------------------
 // Fused residual: strains, return map, trial state, tangent parameters, element nodal
-// forces and Jacobi diagonal contributions.  One CTA per RVE.
+// forces and Jacobi diagonal contributions.  The grid covers all Gauss points of the batch
+// (one thread each, grid-stride in whole waves), whatever RVE they belong to, so an uneven
+// batch keeps every SM busy until the last element; each 8-lane group looks up its RVE.
 template <typename T>
 __global__ void __launch_bounds__(RVE_THREADS) rve_residual_kernel(const RveResidualArgs<T> a) {
-  const int r = blockIdx.x;
-  if (a.active && !a.active[r]) return;
-  const RveDesc d = a.desc[r];
-  const int64_t E = (int64_t)d.nx * d.ny * d.nz;
-  const int64_t G = 8 * E;
-  const double alpha = a.alpha ? a.alpha[r] : 1.0;
-  T ebar[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) ebar[k] = (T)a.macro[6 * r + k];
-  const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
-  const int64_t rounds = (G + blockDim.x - 1) / blockDim.x;
+  const int64_t G_all = 8 * a.nelem;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t rounds = (G_all + stride - 1) / stride;  // the same for every thread (shuffles)
   for (int64_t it = 0; it < rounds; ++it) {
-    const int64_t gl = it * blockDim.x + threadIdx.x;
-    const bool live = gl < G;  // whole 8-lane groups are live or not (G, blockDim multiples of 8)
-    const int64_t le = live ? (gl >> 3) : 0;
+    const int64_t gl = it * stride + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t e = gl < G_all ? (gl >> 3) : 0;  // whole 8-lane groups are in range or not
     const int q = (int)(gl & 7);
+    const int r = rve_of_element(a.desc, a.nrve, e);
+    const RveDesc d = a.desc[r];
+    const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+    const int64_t le = e - d.eoff;
+    const bool live = gl < G_all && le >= 0 && le < E && (!a.active || a.active[r]);
+    const double alpha = a.alpha ? a.alpha[r] : 1.0;
+    T ebar[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ebar[k] = (T)a.macro[6 * r + k];
+    const T jw = (T)(d.hx * d.hy * d.hz / 8.0);
     int i, j, k;
-    local_ijk(d, le, i, j, k);
-    const int64_t e = d.eoff + le;
+    local_ijk(d, live ? le : 0, i, j, k);
     const int64_t g = 8 * e + q;
     double wq[3] = {0.0, 0.0, 0.0};
     if (live) load_w(a.w, a.dw, alpha, element_node(d, i, j, k, q), wq);
@@ -395,8 +397,57 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_residual_kernel(const RveResi
 // ---------------------------------------------------------------------------------------
 // Periodic gather: reduced residual r = T^T f (class 0 removed), Jacobi inverse diagonal,
 // squared norm, class-reaction maximum (class 0 included) and, optionally, the
-// materialised trial fluctuation w_out = w + alpha dw.  One CTA per RVE.
-__global__ void __launch_bounds__(RVE_THREADS) rve_gather_kernel(const RveGatherArgs a) {
+// materialised trial fluctuation w_out = w + alpha dw.  Two kernels: the node pass does the
+// gathers (8 element contributions of f and of the diagonal per periodic node) over a grid
+// that covers every node of the batch, so an uneven batch keeps every SM busy; the norm
+// pass then forms the per-RVE reductions from the gathered residual, one CTA per RVE, in a
+// fixed order (bitwise reproducible).
+__device__ __forceinline__ void gather_node_force(const RveDesc& d, const double* __restrict__ fe,
+                                                  const double* __restrict__ de, int64_t c, double f[3],
+                                                  double dg[3]) {
+  int i, j, k;
+  local_ijk(d, c, i, j, k);
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) f[dd] = dg[dd] = 0.0;
+  for (int n = 0; n < 8; ++n) {
+    const int di = n & 1, dj = (n >> 1) & 1, dk = (n >> 2) & 1;
+    const int ie = (i - di + d.nx) % d.nx, je = (j - dj + d.ny) % d.ny, ke = (k - dk + d.nz) % d.nz;
+    const int64_t e = d.eoff + ie + (int64_t)d.nx * (je + (int64_t)d.ny * ke);
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      f[dd] += fe[(8 * e + n) * 3 + dd];
+      if (de) dg[dd] += de[(8 * e + n) * 3 + dd];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(RVE_THREADS) rve_gather_nodes_kernel(const RveGatherArgs a) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; node < a.nelem; node += stride) {
+    const int r = rve_of_element(a.desc, a.nrve, node);
+    if (a.active && !a.active[r]) continue;
+    const RveDesc d = a.desc[r];
+    const int64_t E = (int64_t)d.nx * d.ny * d.nz;
+    const int64_t c = node - d.eoff;
+    if (c < 0 || c >= E) continue;
+    double f[3], dg[3];
+    gather_node_force(d, a.fe, a.de, c, f, dg);
+    const bool fixed = (c == 0);
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      a.res[3 * node + dd] = fixed ? 0.0 : f[dd];
+      a.dinv[3 * node + dd] = fixed ? 0.0 : 1.0 / dg[dd];
+    }
+    if (a.w_out) {
+      double w[3];
+      load_w(a.w, a.dw, a.alpha ? a.alpha[r] : 1.0, node, w);
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) a.w_out[3 * node + dd] = fixed ? 0.0 : w[dd];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(RVE_THREADS) rve_gather_norms_kernel(const RveGatherArgs a) {
   __shared__ double scratch[32 * 2];
   const int r = blockIdx.x;
   if (a.active && !a.active[r]) return;
@@ -406,35 +457,30 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_gather_kernel(const RveGather
   double acc[2] = {0.0, 0.0};  // ||r||^2, ||w + alpha dw||^2
   double cmax = 0.0;
   for (int64_t c = threadIdx.x; c < E; c += blockDim.x) {
-    int i, j, k;
-    local_ijk(d, c, i, j, k);
-    double f[3] = {0.0, 0.0, 0.0}, dg[3] = {0.0, 0.0, 0.0};
-    for (int n = 0; n < 8; ++n) {
-      const int di = n & 1, dj = (n >> 1) & 1, dk = (n >> 2) & 1;
-      const int ie = (i - di + d.nx) % d.nx, je = (j - dj + d.ny) % d.ny, ke = (k - dk + d.nz) % d.nz;
-      const int64_t e = d.eoff + ie + (int64_t)d.nx * (je + (int64_t)d.ny * ke);
-#pragma unroll
-      for (int dd = 0; dd < 3; ++dd) {
-        f[dd] += a.fe[(8 * e + n) * 3 + dd];
-        dg[dd] += a.de[(8 * e + n) * 3 + dd];
-      }
-    }
     const int64_t node = d.eoff + c;
-    cmax = fmax(cmax, sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]));
+    double f[3];
+    if (c == 0) {  // the eliminated class: its force is not in the reduced residual
+      double dg[3];
+      gather_node_force(d, a.fe, nullptr, 0, f, dg);
+    } else {
 #pragma unroll
-    for (int dd = 0; dd < 3; ++dd) {
-      const bool fixed = (c == 0);
-      a.res[3 * node + dd] = fixed ? 0.0 : f[dd];
-      a.dinv[3 * node + dd] = fixed ? 0.0 : 1.0 / dg[dd];
-      if (!fixed) acc[0] += f[dd] * f[dd];
+      for (int dd = 0; dd < 3; ++dd) f[dd] = a.res[3 * node + dd];
     }
+    cmax = fmax(cmax, sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]));
+    if (c != 0)
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) acc[0] += f[dd] * f[dd];
     double w[3];
-    load_w(a.w, a.dw, alpha, node, w);
+    if (a.w_out) {
+#pragma unroll
+      for (int dd = 0; dd < 3; ++dd) w[dd] = a.w_out[3 * node + dd];
+    } else {
+      load_w(a.w, a.dw, alpha, node, w);
+    }
 #pragma unroll
     for (int dd = 0; dd < 3; ++dd) {
       const double wv = (c == 0) ? 0.0 : w[dd];
       acc[1] += wv * wv;
-      if (a.w_out) a.w_out[3 * node + dd] = wv;
     }
   }
   block_sum<2>(acc, scratch);
@@ -601,7 +647,7 @@ __global__ void __launch_bounds__(RVE_THREADS, 2) rve_pcg_kernel(const RvePcgArg
   block_sum<2>(v, scratch);
   double rz = v[0];
   const double bnorm = sqrt(v[1]);
-  const double tol = a.rtol * bnorm;
+  const double tol = (a.rtol_dev ? *a.rtol_dev : a.rtol) * bnorm;
   int status = 1, iters = 0;
   double rnorm = bnorm;
   if (bnorm == 0.0 || !(bnorm == bnorm)) {
@@ -843,7 +889,7 @@ __global__ void __launch_bounds__(RVE_THREADS, sizeof(T) == 4 ? 2 : 1) rve_pcg_c
   cluster_sum<2>(v, scratch, slot_init, cl);  // its barrier also publishes p
   double rz = v[0];
   const double bnorm = sqrt(v[1]);
-  const double tol = a.rtol * bnorm;
+  const double tol = (a.rtol_dev ? *a.rtol_dev : a.rtol) * bnorm;
   int status = 1, iters = 0;
   double rnorm = bnorm;
   if (bnorm == 0.0 || !(bnorm == bnorm)) {
@@ -1284,12 +1330,21 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_response_kernel(const RveResp
 
 template <typename T>
 int launch_rve_residual(const RveResidualArgs<T>& a, int nrve, cudaStream_t st) {
-  rve_residual_kernel<T><<<nrve, RVE_THREADS, 0, st>>>(a);
+  (void)nrve;
+  if (a.nelem <= 0) return CIB_OK;
+  const int grid = persistent_grid(reinterpret_cast<const void*>(rve_residual_kernel<T>), RVE_THREADS, 8 * a.nelem);
+  rve_residual_kernel<T><<<grid, RVE_THREADS, 0, st>>>(a);
   return check_launch();
 }
 
 int launch_rve_gather(const RveGatherArgs& a, int nrve, cudaStream_t st) {
-  rve_gather_kernel<<<nrve, RVE_THREADS, 0, st>>>(a);
+  if (a.nelem > 0) {
+    const int grid = persistent_grid(reinterpret_cast<const void*>(rve_gather_nodes_kernel), RVE_THREADS, a.nelem);
+    rve_gather_nodes_kernel<<<grid, RVE_THREADS, 0, st>>>(a);
+    const int rc = check_launch();
+    if (rc != CIB_OK) return rc;
+  }
+  rve_gather_norms_kernel<<<nrve, RVE_THREADS, 0, st>>>(a);
   return check_launch();
 }
 

@@ -56,6 +56,8 @@ struct PhaseTable {
 template <typename T>
 struct RveResidualArgs {
   const RveDesc* desc;
+  int nrve;
+  int64_t nelem;  // elements of the batch (RVE r owns [desc[r].eoff, desc[r].eoff + E_r))
   const uint8_t* phase;
   PhaseTable<T> mats;
   const double* macro;
@@ -81,6 +83,8 @@ struct RveResidualArgs {
 
 struct RveGatherArgs {
   const RveDesc* desc;
+  int nrve;
+  int64_t nelem;
   const double* fe;
   const double* de;
   const double* w;
@@ -113,6 +117,7 @@ struct RvePcgArgs {
   double* p;
   double* Ap;
   double rtol;
+  const double* rtol_dev = nullptr;  // when set, the relative tolerance is read here (device-side control)
   int maxit;
   int32_t* status;
   int32_t* iterations;
@@ -172,6 +177,131 @@ struct RveResponseArgs {
   double* point_out;
   double* diag;
 };
+
+// ---------------------------------------------------------------------------------------
+// Host-side argument builders from the public batch struct (shared by the C entry points).
+
+template <typename T>
+inline PhaseTable<T> rve_phase_table(const cib_rve_batch& b) {
+  PhaseTable<T> t;
+  for (int i = 0; i < RVE_MAX_PHASES; ++i) {
+    const cib_phase_material& pm = b.mats[i < b.nphase ? i : 0];
+    PhaseMat<T>& m = t.m[i];
+    m.kind = pm.kind;
+    cib_j2vp_material params = pm.params;
+    if (pm.kind == PHASE_ELASTIC) {
+      // elastic phases only use the elasticity entries; keep the J2 block well defined
+      params.yield_stress = 1.0;
+      params.time_scale = 1.0;
+      params.reference_stress = 1.0;
+      params.rate_exponent = 1.0;
+    }
+    m.j2 = make_j2_consts<T>(params, b.settings);
+    m.C11 = m.j2.C11;
+    m.C12 = m.j2.C12;
+    m.G = m.j2.G;
+    m.K = m.j2.K;
+  }
+  return t;
+}
+
+template <typename T>
+inline RveResidualArgs<T> rve_residual_args(const cib_rve_batch& b, const double* dt, const double* macro,
+                                            const double* w, const double* dw, const double* alpha,
+                                            const int32_t* active, unsigned long long* fail) {
+  RveResidualArgs<T> a;
+  a.desc = reinterpret_cast<const RveDesc*>(b.desc);
+  a.nrve = b.nrve;
+  a.nelem = b.nelem;
+  a.phase = b.phase;
+  a.mats = rve_phase_table<T>(b);
+  a.macro = macro;
+  a.w = w;
+  a.dw = dw;
+  a.alpha = alpha;
+  a.active = active;
+  a.ngp = 8 * b.nelem;
+  a.ep_n = static_cast<const T*>(b.plastic_strain_n);
+  a.q_n = b.eqps_n;
+  a.vpm_n = b.vpm_n;
+  a.ep = static_cast<T*>(b.plastic_strain);
+  a.q = b.eqps;
+  a.vpm = b.vpm;
+  a.stress = static_cast<T*>(b.stress);
+  a.tparam = static_cast<T*>(b.tparam);
+  a.tflag = b.tflag;
+  a.fe = b.fe;
+  a.de = b.de;
+  a.dt = dt;
+  a.fail = fail;
+  return a;
+}
+
+inline RveGatherArgs rve_gather_args(const cib_rve_batch& b, const double* w, const double* dw, const double* alpha,
+                                     const int32_t* active, double* residual, double* dinv, double* rnorm2,
+                                     double* wnorm2, double* class_max, double* w_out) {
+  RveGatherArgs a;
+  a.desc = reinterpret_cast<const RveDesc*>(b.desc);
+  a.nrve = b.nrve;
+  a.nelem = b.nelem;
+  a.fe = b.fe;
+  a.de = b.de;
+  a.w = w;
+  a.dw = dw;
+  a.alpha = alpha;
+  a.active = active;
+  a.res = residual;
+  a.dinv = dinv;
+  a.rnorm2 = rnorm2;
+  a.wnorm2 = wnorm2;
+  a.class_max = class_max;
+  a.w_out = w_out;
+  return a;
+}
+
+template <typename T>
+inline RvePcgArgs<T> rve_pcg_args(const cib_rve_batch& b, const int32_t* sys_rve, const int64_t* sys_off,
+                                  const int32_t* active, const double* rhs, const double* dinv, double* x, double* r,
+                                  double* p, double* Ap, double rtol, int32_t maxit, int32_t* status,
+                                  int32_t* iterations, double* rel, double* xnorm) {
+  RvePcgArgs<T> a;
+  a.desc = reinterpret_cast<const RveDesc*>(b.desc);
+  a.phase = b.phase;
+  a.mats = rve_phase_table<T>(b);
+  a.ngp = 8 * b.nelem;
+  a.tparam = static_cast<const T*>(b.tparam);
+  a.tflag = b.tflag;
+  a.sys_rve = sys_rve;
+  a.sys_off = sys_off;
+  a.active = active;
+  a.b = rhs;
+  a.dinv = dinv;
+  a.x = x;
+  a.r = r;
+  a.p = p;
+  a.Ap = Ap;
+  a.rtol = rtol;
+  a.maxit = maxit;
+  a.status = status;
+  a.iterations = iterations;
+  a.rel_residual = rel;
+  a.xnorm = xnorm;
+  return a;
+}
+
+// RVE owning batch element (or periodic node) e: the last r with desc[r].eoff <= e (RVEs
+// are stored in element order).  A binary search over the descriptors, which stay in L1.
+__device__ __forceinline__ int rve_of_element(const RveDesc* __restrict__ desc, int nrve, int64_t e) {
+  int lo = 0, hi = nrve - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&desc[mid].eoff) <= e)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
 
 template <typename T>
 int launch_rve_residual(const RveResidualArgs<T>& a, int nrve, cudaStream_t st);

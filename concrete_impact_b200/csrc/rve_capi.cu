@@ -7,30 +7,6 @@
 namespace cib {
 namespace {
 
-template <typename T>
-PhaseTable<T> make_table(const cib_rve_batch& b) {
-  PhaseTable<T> t;
-  for (int i = 0; i < RVE_MAX_PHASES; ++i) {
-    const cib_phase_material& pm = b.mats[i < b.nphase ? i : 0];
-    PhaseMat<T>& m = t.m[i];
-    m.kind = pm.kind;
-    cib_j2vp_material params = pm.params;
-    if (pm.kind == PHASE_ELASTIC) {
-      // elastic phases only use the elasticity entries; keep the J2 block well defined
-      params.yield_stress = 1.0;
-      params.time_scale = 1.0;
-      params.reference_stress = 1.0;
-      params.rate_exponent = 1.0;
-    }
-    m.j2 = make_j2_consts<T>(params, b.settings);
-    m.C11 = m.j2.C11;
-    m.C12 = m.j2.C12;
-    m.G = m.j2.G;
-    m.K = m.j2.K;
-  }
-  return t;
-}
-
 bool batch_ok(const cib_rve_batch* b) {
   return b && b->nrve >= 0 && b->nphase >= 1 && b->nphase <= RVE_MAX_PHASES && b->nelem >= 0 && b->desc &&
          b->phase && (b->precision == 32 || b->precision == 64);
@@ -39,30 +15,7 @@ bool batch_ok(const cib_rve_batch* b) {
 template <typename T>
 int residual_t(const cib_rve_batch& b, const double* dt, const double* macro, const double* w, const double* dw,
                const double* alpha, const int32_t* active, unsigned long long* fail, cudaStream_t st) {
-  RveResidualArgs<T> a;
-  a.desc = reinterpret_cast<const RveDesc*>(b.desc);
-  a.phase = b.phase;
-  a.mats = make_table<T>(b);
-  a.macro = macro;
-  a.w = w;
-  a.dw = dw;
-  a.alpha = alpha;
-  a.active = active;
-  a.ngp = 8 * b.nelem;
-  a.ep_n = static_cast<const T*>(b.plastic_strain_n);
-  a.q_n = b.eqps_n;
-  a.vpm_n = b.vpm_n;
-  a.ep = static_cast<T*>(b.plastic_strain);
-  a.q = b.eqps;
-  a.vpm = b.vpm;
-  a.stress = static_cast<T*>(b.stress);
-  a.tparam = static_cast<T*>(b.tparam);
-  a.tflag = b.tflag;
-  a.fe = b.fe;
-  a.de = b.de;
-  a.dt = dt;
-  a.fail = fail;
-  return launch_rve_residual<T>(a, b.nrve, st);
+  return launch_rve_residual<T>(rve_residual_args<T>(b, dt, macro, w, dw, alpha, active, fail), b.nrve, st);
 }
 
 template <typename T>
@@ -70,28 +23,8 @@ int pcg_t(const cib_rve_batch& b, int32_t nsys, const int32_t* sys_rve, const in
           const double* rhs, const double* dinv, double* x, double* r, double* p, double* Ap, double rtol,
           int32_t maxit, int32_t* status, int32_t* iterations, double* rel, double* xnorm, cudaStream_t st,
           int32_t cluster = 1) {
-  RvePcgArgs<T> a;
-  a.desc = reinterpret_cast<const RveDesc*>(b.desc);
-  a.phase = b.phase;
-  a.mats = make_table<T>(b);
-  a.ngp = 8 * b.nelem;
-  a.tparam = static_cast<const T*>(b.tparam);
-  a.tflag = b.tflag;
-  a.sys_rve = sys_rve;
-  a.sys_off = sys_off;
-  a.active = active;
-  a.b = rhs;
-  a.dinv = dinv;
-  a.x = x;
-  a.r = r;
-  a.p = p;
-  a.Ap = Ap;
-  a.rtol = rtol;
-  a.maxit = maxit;
-  a.status = status;
-  a.iterations = iterations;
-  a.rel_residual = rel;
-  a.xnorm = xnorm;
+  const RvePcgArgs<T> a = rve_pcg_args<T>(b, sys_rve, sys_off, active, rhs, dinv, x, r, p, Ap, rtol, maxit, status,
+                                          iterations, rel, xnorm);
   return launch_rve_pcg_cluster<T>(a, nsys, b.max_nxy, cluster, st);
 }
 
@@ -101,7 +34,7 @@ int tangent_rhs_t(const cib_rve_batch& b, const int32_t* active, double* fe6, do
   RveTangentArgs<T> a;
   a.desc = reinterpret_cast<const RveDesc*>(b.desc);
   a.phase = b.phase;
-  a.mats = make_table<T>(b);
+  a.mats = rve_phase_table<T>(b);
   a.ngp = 8 * b.nelem;
   a.ne_total = b.nelem;
   a.tparam = static_cast<const T*>(b.tparam);
@@ -120,8 +53,8 @@ int response_t(const cib_rve_batch& b, const double* dt, const double* macro, co
   RveResponseArgs<T> a;
   a.desc = reinterpret_cast<const RveDesc*>(b.desc);
   a.phase = b.phase;
-  a.mats = make_table<double>(b);
-  a.mats_t = make_table<T>(b);
+  a.mats = rve_phase_table<double>(b);
+  a.mats_t = rve_phase_table<T>(b);
   a.macro = macro;
   a.macro_n = macro_n;
   a.w = w;
@@ -165,20 +98,8 @@ extern "C" int cib_rve_gather(const cib_rve_batch* batch, const double* w, const
                               double* wnorm2, double* class_max, double* w_out, void* stream) {
   if (!batch_ok(batch) || !w || !residual || !dinv || !rnorm2 || !batch->fe || !batch->de) return CIB_EINVAL;
   if (batch->nrve == 0) return CIB_OK;
-  RveGatherArgs a;
-  a.desc = reinterpret_cast<const RveDesc*>(batch->desc);
-  a.fe = batch->fe;
-  a.de = batch->de;
-  a.w = w;
-  a.dw = dw;
-  a.alpha = alpha;
-  a.active = active;
-  a.res = residual;
-  a.dinv = dinv;
-  a.rnorm2 = rnorm2;
-  a.wnorm2 = wnorm2;
-  a.class_max = class_max;
-  a.w_out = w_out;
+  const RveGatherArgs a = rve_gather_args(*batch, w, dw, alpha, active, residual, dinv, rnorm2, wnorm2, class_max,
+                                          w_out);
   return launch_rve_gather(a, batch->nrve, reinterpret_cast<cudaStream_t>(stream));
 }
 

@@ -95,29 +95,6 @@ int work_address(double** out) {
 }
 
 template <typename T>
-PhaseTable<T> table_of(const cib_rve_batch& b) {
-  PhaseTable<T> t;
-  for (int i = 0; i < RVE_MAX_PHASES; ++i) {
-    const cib_phase_material& pm = b.mats[i < b.nphase ? i : 0];
-    PhaseMat<T>& m = t.m[i];
-    m.kind = pm.kind;
-    cib_j2vp_material params = pm.params;
-    if (pm.kind == PHASE_ELASTIC) {
-      params.yield_stress = 1.0;
-      params.time_scale = 1.0;
-      params.reference_stress = 1.0;
-      params.rate_exponent = 1.0;
-    }
-    m.j2 = make_j2_consts<T>(params, b.settings);
-    m.C11 = m.j2.C11;
-    m.C12 = m.j2.C12;
-    m.G = m.j2.G;
-    m.K = m.j2.K;
-  }
-  return t;
-}
-
-template <typename T>
 int solve(const cib_rve_batch& b, int32_t nsys, const int32_t* sys_rve, const int64_t* sys_off,
           const int32_t* active, int64_t vec_len, double* work, const double* rhs, const double* dinv, double* x,
           double rtol, int32_t maxit, int32_t* status, int32_t* iterations, double* rel, double* xnorm,
@@ -125,7 +102,7 @@ int solve(const cib_rve_batch& b, int32_t nsys, const int32_t* sys_rve, const in
   RvePcgArgs<T> a;
   a.desc = reinterpret_cast<const RveDesc*>(b.desc);
   a.phase = b.phase;
-  a.mats = table_of<T>(b);
+  a.mats = rve_phase_table<T>(b);
   a.ngp = 8 * b.nelem;
   a.tparam = static_cast<const T*>(b.tparam);
   a.tflag = b.tflag;

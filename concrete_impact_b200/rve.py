@@ -363,10 +363,13 @@ class RVEBatch:
     All RVEs share the phase materials (same model family) but may differ in divisions and
     lengths.  State arrays are SoA over all Gauss points; periodic vectors are float64.
     ``precision`` 64 or 32 selects the element arithmetic (history stays float64).
+    ``device_control`` runs each Newton solve without Armijo search as one CUDA graph whose
+    iterations are decided on the device (``cib_rve_newton_graph_*``): one launch and one
+    read-back per step instead of two host round trips per Newton iteration.
     """
 
     def __init__(self, models: list[StructuredHex8RVE], precision: int = 64,
-                 linear_solver: LinearSolverOptions | None = None) -> None:  # fmt: skip
+                 linear_solver: LinearSolverOptions | None = None, device_control: bool = False) -> None:  # fmt: skip
         if not models:
             raise ValueError("an RVE batch needs at least one model")
         self.device = _native.require_cuda()
@@ -444,6 +447,9 @@ class RVEBatch:
         c = self.linear.cluster
         self.cluster = auto_pcg_cluster(self) if c == "auto" else self.check_cluster(int(c))
         self._batch_struct = None
+        self.device_control = bool(device_control)
+        self.live_mask = torch.ones(self.nrve, dtype=torch.int32, device=dev)
+        self._graphs: dict = {}
 
     # -- C structs ---------------------------------------------------------------------
     def batch_struct(self, settings: MaterialUpdateSettings) -> _native.RVEBatchC:
@@ -542,6 +548,17 @@ class RVEBatch:
         )  # fmt: skip
         _native.check(code, "cib_rve_response")
 
+    def newton_graph(self, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings) -> "_NewtonGraph":
+        """The device-controlled Newton graph for these settings (built once, then reused;
+        the PCG cluster size and tolerances in force are part of the key)."""
+        key = (tuple(_newton_key(newton)), repr(update_settings), self.cluster, float(self.rtol),
+               int(self.linear.max_iterations), self.linear.forcing)  # fmt: skip
+        graph = self._graphs.get(key)
+        if graph is None:
+            graph = _NewtonGraph(self, newton, update_settings)
+            self._graphs[key] = graph
+        return graph
+
     def save_state(self, path) -> None:
         """Write the committed state of every RVE (history, fluctuation, macro strain) to an
         .npz file, for resuming long runs."""
@@ -564,6 +581,100 @@ class RVEBatch:
         self.vpm_n.copy_(self.vpm)
         self.w_n.copy_(self.w)
         self.macro_n.copy_(self.macro)
+
+
+# --------------------------------------------------------------------------------------
+# Device-controlled Newton solve: one CUDA graph per step (csrc/rve_newton.cu).
+
+_CTL = 16  # control words ahead of the per-RVE records in the graph's workspaces
+
+
+def _newton_key(newton: NonlinearNewtonSettings) -> list:
+    return [int(newton.max_iterations), float(newton.residual_absolute_tolerance),
+            float(newton.residual_relative_tolerance), float(newton.increment_absolute_tolerance),
+            float(newton.increment_relative_tolerance)]  # fmt: skip
+
+
+class _NewtonGraph:
+    """Workspaces and the instantiated graph of ``cib_rve_newton_graph_create``."""
+
+    def __init__(self, batch: RVEBatch, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings) -> None:
+        lib = batch.lib
+        n_int, n_double = ctypes.c_int64(), ctypes.c_int64()
+        lib.cib_rve_newton_workspace(batch.nrve, ctypes.byref(n_int), ctypes.byref(n_double))
+        dev = batch.device
+        self.iwork = torch.zeros(n_int.value, dtype=torch.int32, device=dev)
+        self.dwork = torch.zeros(n_double.value, dtype=torch.float64, device=dev)
+        self.batch = batch
+        self.b = batch.batch_struct(update_settings)
+        s = _native.RVENewtonC()
+        s.max_iterations = int(newton.max_iterations)
+        s.inexact = 1 if batch.linear.forcing == "eisenstat_walker" else 0
+        s.residual_absolute_tolerance = float(newton.residual_absolute_tolerance)
+        s.residual_relative_tolerance = float(newton.residual_relative_tolerance)
+        s.increment_absolute_tolerance = float(newton.increment_absolute_tolerance)
+        s.increment_relative_tolerance = float(newton.increment_relative_tolerance)
+        s.pcg_rtol = float(batch.rtol)
+        s.pcg_maxit = int(batch.linear.max_iterations)
+        s.cluster = int(batch.cluster)
+        for name, tensor in (("time_step", batch.dt), ("macro", batch.macro), ("w_n", batch.w_n), ("w", batch.w),
+                             ("w_out", batch.w_out), ("x", batch.x), ("r", batch.r), ("p", batch.p), ("Ap", batch.Ap),
+                             ("residual", batch.res), ("dinv", batch.dinv), ("rnorm2", batch.rnorm2),
+                             ("wnorm2", batch.wnorm2), ("class_max", batch.class_max), ("alpha", batch.alpha),
+                             ("active", batch.active), ("live_mask", batch.live_mask), ("fail", batch.fail),
+                             ("sys_rve", batch.sys_rve), ("sys_off", batch.sys_off), ("pcg_status", batch.pcg_status),
+                             ("pcg_iterations", batch.pcg_iters), ("pcg_rel_residual", batch.pcg_rel),
+                             ("pcg_xnorm", batch.pcg_xnorm), ("iwork", self.iwork), ("dwork", self.dwork)):  # fmt: skip
+            setattr(s, name, tensor.data_ptr())
+        self.struct = s
+        handle = ctypes.c_void_p()
+        torch.cuda.synchronize()
+        _native.check(lib.cib_rve_newton_graph_create(ctypes.byref(self.b), ctypes.byref(s), ctypes.byref(handle)),
+                      "cib_rve_newton_graph_create")  # fmt: skip
+        self.handle = handle
+        self.lib = lib
+
+    def launch(self) -> None:
+        _native.check(self.lib.cib_rve_newton_graph_launch(self.handle, _native.stream_ptr()),
+                      "cib_rve_newton_graph_launch")  # fmt: skip
+
+    def __del__(self) -> None:
+        handle = getattr(self, "handle", None)
+        if handle is not None and handle.value:
+            self.lib.cib_rve_newton_graph_destroy(handle)
+            self.handle = None
+
+
+def _solve_batch_step_graph(batch: RVEBatch, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings,
+                            failure_context, live_mask) -> BatchStepResult:  # fmt: skip
+    """solve_batch_step on the device: one graph launch, one read-back of the records."""
+    R = batch.nrve
+    graph = batch.newton_graph(newton, update_settings)
+    if live_mask is None:
+        batch.live_mask.fill_(1)
+    else:
+        batch.live_mask.copy_(torch.as_tensor(np.asarray(live_mask, dtype=np.int32), device=batch.device))
+    graph.launch()
+    iw = graph.iwork.cpu().numpy()
+    dw = graph.dwork.cpu().numpy()
+    its, pcg = iw[_CTL : _CTL + R].astype(np.int64), iw[_CTL + R : _CTL + 2 * R].astype(np.int64)
+    rnorm, tol = dw[_CTL : _CTL + R], dw[_CTL + R : _CTL + 2 * R]
+    inc, inc_tol = dw[_CTL + 2 * R : _CTL + 3 * R], dw[_CTL + 3 * R : _CTL + 4 * R]
+    error, r, info = int(iw[1]), int(iw[2]), int(iw[3])
+    if error == 1:
+        if failure_context is not None:
+            raise failure_context(r, info)
+        raise MaterialPointConvergenceError("RVE material point failed.", "material_point_failure",
+                                            {"rve_index": r, "point_id": info})  # fmt: skip
+    if error == 3:
+        raise RVEEquilibriumError("maximum_iterations_exceeded", _failure_diag(batch, r, int(iw[0]), rnorm[r], tol[r],
+                                                                               inc[r], inc_tol[r]))  # fmt: skip
+    if error == 2:
+        d = _failure_diag(batch, r, int(iw[0]) - 1, rnorm[r], tol[r], float(inc[r]), inc_tol[r])
+        d["linear_solver_status"] = info
+        raise RVEEquilibriumError("non_finite_increment", d)
+    live = np.ones(R, dtype=bool) if live_mask is None else np.asarray(live_mask, dtype=bool)
+    return BatchStepResult(its, np.zeros(R, dtype=np.int64), np.where(live, rnorm, 0.0), np.where(live, tol, 0.0), pcg)
 
 
 # --------------------------------------------------------------------------------------
@@ -603,6 +714,8 @@ def solve_batch_step(
     ``timers``, when given, collects CUDA event pairs around the residual and PCG launches
     (keys "residual", "pcg"; read them after a synchronize).
     """
+    if batch.device_control and not newton.armijo.enabled and timers is None:
+        return _solve_batch_step_graph(batch, newton, update_settings, failure_context, live_mask)
     R = batch.nrve
     b = batch.batch_struct(update_settings)
     batch.w.copy_(batch.w_n)

@@ -211,7 +211,8 @@ int cib_csr_gather(int64_t nnz, const int64_t* ptr, const int64_t* list, const d
 
 /* --- Periodic structured Hex8 RVE batch ------------------------------------------------
  * A batch holds R structured periodic RVEs (unit-cell boxes of nx*ny*nz Hex8 elements).
- * RVE r owns elements [elem_offset, elem_offset + nx*ny*nz); its periodic node (class)
+ * RVE r owns elements [elem_offset, elem_offset + nx*ny*nz), the RVEs one after the other
+ * (elem_offset ascending, RVE 0 at 0, the last ending at nelem); its periodic node (class)
  * c = i + nx*(j + ny*k) is batch node elem_offset + c; class 0 is the eliminated
  * reference class (src/fem/rve/periodic.py:20-104).  Periodic vectors (fluctuation w,
  * residual, PCG vectors) are float64 with 3 entries per batch node.  Gauss-point arrays
@@ -336,6 +337,67 @@ int cib_rve_tangent_finish(const cib_rve_batch* batch, const int32_t* active, co
 int cib_rve_response(const cib_rve_batch* batch, const double* time_step, const double* macro, const double* macro_n,
                      const double* w, const double* w_n, const int32_t* active, double* sums, double* point_out,
                      double* diagnostics, void* stream);
+
+/* Device-controlled batched Newton solve of every RVE of a batch from its committed state
+ * (solver.py:62-227 without the Armijo search): the residual and increment tests, the
+ * per-RVE convergence and live masks, the Eisenstat-Walker forcing of the PCG tolerance
+ * (inexact != 0: eta = 0.9 (max live ||r_k|| / ||r_k-1||)^2 with its safeguard, at most
+ * 0.1, at least pcg_rtol) and the update w += -dw run on the device.  The whole solve is
+ * one CUDA graph: w = w_n, then a conditional WHILE node whose body is residual, gather,
+ * convergence check, PCG, increment check and update, repeated until every live RVE has
+ * converged or an error stopped it -- no host round trip inside a step.  Afterwards the
+ * trial state of every RVE is its converged state and active = live_mask.
+ * Outputs in iwork / dwork (sizes from cib_rve_newton_workspace; layout below):
+ *   iwork[0] iterations run, [1] error (0 none, 1 material point failure, 2 non-finite
+ *   increment, 3 maximum iterations), [2] failing RVE, [3] failing local point or PCG
+ *   status, [16 + r] Newton iterations of RVE r, [16 + R + r] PCG iterations of RVE r;
+ *   dwork[16 + r] residual norm, [16 + R + r] residual tolerance, [16 + 2R + r] increment
+ *   norm, [16 + 3R + r] increment tolerance (at the last check).
+ * All pointers are device memory of the batch's buffers (the same meaning as in
+ * cib_rve_residual, cib_rve_gather and cib_rve_pcg_cluster). */
+typedef struct cib_rve_newton {
+  int32_t max_iterations;
+  int32_t inexact;
+  double residual_absolute_tolerance;
+  double residual_relative_tolerance;
+  double increment_absolute_tolerance;
+  double increment_relative_tolerance;
+  double pcg_rtol;
+  int32_t pcg_maxit;
+  int32_t cluster; /* PCG CTAs per system: 1, 2, 4 or 8 */
+  const double* time_step;
+  const double* macro;
+  const double* w_n;
+  double* w;
+  double* w_out;
+  double* x;
+  double* r;
+  double* p;
+  double* Ap;
+  double* residual;
+  double* dinv;
+  double* rnorm2;
+  double* wnorm2;
+  double* class_max;
+  double* alpha;
+  int32_t* active;
+  const int32_t* live_mask; /* RVEs to solve; the others keep w = w_n and stay inactive */
+  unsigned long long* fail;
+  const int32_t* sys_rve;
+  const int64_t* sys_off;
+  int32_t* pcg_status;
+  int32_t* pcg_iterations;
+  double* pcg_rel_residual;
+  double* pcg_xnorm;
+  int32_t* iwork;
+  double* dwork;
+} cib_rve_newton;
+void cib_rve_newton_workspace(int32_t nrve, int64_t* n_int, int64_t* n_double);
+/* Build the graph (captured on a private stream; the batch struct and the settings are
+ * baked in, so a change of either needs a new graph).  *graph receives an opaque handle. */
+int cib_rve_newton_graph_create(const cib_rve_batch* batch, const cib_rve_newton* newton, void** graph);
+int cib_rve_newton_graph_launch(void* graph, void* stream);
+int cib_rve_newton_graph_destroy(void* graph);
 
 /* --- Tensor-core MLP GEMM (recurrent material surrogate) --------------------------------
  * C[M x N] = A[M x K] . B[N x K]^T, A and B bf16 row-major (leading dimensions lda, ldb,

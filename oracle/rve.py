@@ -124,8 +124,8 @@ class RVEOracle:
     def assemble(self, u, u_prev, dt, state):
         ue = u[self.dofs]
         up = u_prev[self.dofs]
-        eps = np.einsum("eqij,ej->eqi", self.b, ue).reshape(-1, 6)
-        rate = (np.einsum("eqij,ej->eqi", self.b, ue - up) / dt).reshape(-1, 6)
+        eps = np.matmul(self.b, ue[:, None, :, None])[..., 0].reshape(-1, 6)
+        rate = (np.matmul(self.b, (ue - up)[:, None, :, None])[..., 0] / dt).reshape(-1, 6)
         n = self.n_gp
         stress, tangent = np.zeros((n, 6)), np.zeros((n, 6, 6))
         psi, diss = np.zeros(n), np.zeros(n)
@@ -159,10 +159,13 @@ class RVEOracle:
         E = self.elements.shape[0]
         s4 = stress.reshape(E, 8, 6)
         t4 = tangent.reshape(E, 8, 6, 6)
-        fe = np.einsum("eqij,eqi,eq->ej", self.b, s4, self.jw)
+        fe = np.einsum("eqij,eqi,eq->ej", self.b, s4, self.jw, optimize=True)
         f = np.zeros(u.size)
         np.add.at(f, self.dofs.ravel(), fe.ravel())
-        ke = np.einsum("eqki,eqkl,eqlj,eq->eij", self.b, t4, self.b, self.jw)
+        # K_e = sum_q w B^T C B: batched products (the same sum as the reference's per-element
+        # loop, in a different floating-point order)
+        cb = np.matmul(t4, self.b)  # (E, 8, 6, 24)
+        ke = np.einsum("eqki,eqkj,eq->eij", self.b, cb, self.jw, optimize=True)
         k = coo_matrix((ke.ravel(), (self.rows, self.cols)), shape=(u.size, u.size)).tocsr()
         return {"f": f, "K": k, "eps": eps, "rate": rate, "stress": stress, "psi": psi, "diss": diss, "state": new,
                 "iwd": iwd, "active": active, "margin": margin}  # fmt: skip

@@ -18,6 +18,7 @@ import json
 import os
 import sys
 import tempfile
+import time
 from pathlib import Path
 
 import numpy as np
@@ -177,6 +178,132 @@ def _rve_arrays(prefix: str, response, macro) -> dict:
     scalars["free_energy_density"] = response.free_energy_density
     scalars["dissipation_density"] = response.dissipation_density
     return out, scalars
+
+
+# Uneven RVE batch of the 256-RVE workload: per RVE i, edge drawn from EDGES with seed
+# 1000 + i, sphere layout seed i, random 4-segment macro path seed 5000 + i (200 steps).
+# The golden RVEs are the first workload RVE of each edge, advanced over coarse steps of
+# their own paths (time indices 0, 10, 20, 30) so that the mortar yields.
+RVE_BATCH_EDGES = (8, 12, 16, 20, 24)
+RVE_BATCH_TIME_INDICES = (0, 10, 20, 30)
+
+
+def rve_batch_golden_members() -> list[tuple[int, int]]:
+    """(workload RVE index, edge) of the first RVE of each edge of the 256-RVE workload."""
+    found = {}
+    for i in range(256):
+        edge = int(np.random.default_rng(1000 + i).choice(RVE_BATCH_EDGES))
+        found.setdefault(edge, i)
+    return [(found[e], e) for e in RVE_BATCH_EDGES]
+
+
+def make_rve_batch_cases():
+    """The reference's solve_rve_microequilibrium (FP64, direct solves) on one RVE of each
+    edge of the uneven 256-RVE workload, along its own macro path; homogenised stress and
+    Newton iterations per step."""
+    from fem.materials.linear_elastic import LinearElasticMaterial
+    from fem.materials.phased import PhasedMaterialModel, RVEPhase
+    from fem.materials.plasticity import J2ViscoplasticMaterial
+    from fem.mesh.structured import build_structured_hex8_box
+    from fem.rve import (RVERequest, StructuredHex8RVE, build_structured_hex8_periodic_constraint,
+                         initialize_rve_state, solve_rve_microequilibrium)  # fmt: skip
+    from fem.solvers.data import ArmijoSettings, NonlinearNewtonSettings
+    from fem.materials.data import MaterialUpdateSettings
+
+    sys.path.insert(0, str(REPO))
+    from concrete_impact_b200.rve_builders import draw_spheres, random_strain_path, sphere_phase_map
+
+    update = MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10)
+    mortar = J2ViscoplasticMaterial("mortar", 2200.0, 25.0e9, 0.2, 20.0e6, 2.0e9, 1.0e-3, 20.0e6, 1.0)
+    aggregate = LinearElasticMaterial("aggregate", 2600.0, 50.0e9, 0.2)
+    newton = NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=False))
+    cases = {}
+    for index, edge in rve_batch_golden_members():
+        div = (edge, edge, edge)
+        nodes, elements = build_structured_hex8_box((1.0, 1.0, 1.0), div)
+        phase = sphere_phase_map(div, draw_spheres(index))
+        phased = PhasedMaterialModel("mortar__aggregate", (RVEPhase("matrix", mortar), RVEPhase("inclusion", aggregate)),
+                                     np.repeat(phase, 8), 2360.0)  # fmt: skip
+        model = StructuredHex8RVE(nodes, elements, div, phased, build_structured_hex8_periodic_constraint(nodes, div),
+                                  newton, element_phase_ids=phase, phase_names=("matrix", "inclusion"))  # fmt: skip
+        times, strains = random_strain_path(5000 + index, 200, 4, 1.0e-2, (1.0, 1000.0))
+        ti = np.asarray(RVE_BATCH_TIME_INDICES)
+        state = initialize_rve_state(model)
+        stress, newton_its, active, eqps = [], [], [], []
+        t0 = time.perf_counter()
+        for a, b in zip(ti[:-1], ti[1:]):
+            response = solve_rve_microequilibrium(model, RVERequest(strains[b], float(times[b] - times[a]), update),
+                                                  state)  # fmt: skip
+            stress.append(response.macro_stress)
+            newton_its.append(int(response.diagnostics["newton_iterations"]))
+            active.append(float(response.diagnostics.get("viscoplastic_active_volume_fraction", np.nan)))
+            eqps.append(float(np.mean(response.state.material_state.variables["phase_matrix__equivalent_plastic_strain"])))
+            state = response.state
+        seconds = time.perf_counter() - t0
+        print(f"rve_batch edge {edge} (RVE {index}): {seconds:.1f} s", flush=True)
+        arrays = {"element_phase": phase.astype(np.uint8), "macro_strain": strains[ti[1:]],
+                  "time_step": np.diff(times[ti]), "macro_stress": np.asarray(stress)}  # fmt: skip
+        meta = {"kind": "rve_batch_member", "workload_index": index, "edge": edge, "layout_seed": index,
+                "path_seed": 5000 + index, "time_indices": list(RVE_BATCH_TIME_INDICES),
+                "newton_iterations": newton_its, "mean_matrix_eqps": eqps, "active_fraction": active,
+                "newton": [25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, False], "reference_seconds": seconds}  # fmt: skip
+        cases[f"rve_batch_edge{edge}"] = (arrays, meta)
+    return cases
+
+
+def make_rve_path_cases(steps: int = 30):
+    """The mixed-control uniaxial compression path of the 8^3 concrete RVE (seed 0): xx
+    strain ramped to -0.5 % in 100 steps at 10 /s, the other components free at zero
+    macro stress.  The outer iteration is this package's harness loop
+    (rve_builders.solve_mixed_control_step, which corrects the free components with the
+    effective tangent); every RVE solve inside it is the reference's
+    solve_rve_microequilibrium with its effective tangent.  First ``steps`` steps."""
+    from fem.materials.data import MaterialResponseRequirements, MaterialUpdateSettings
+    from fem.materials.linear_elastic import LinearElasticMaterial
+    from fem.materials.phased import PhasedMaterialModel, RVEPhase
+    from fem.materials.plasticity import J2ViscoplasticMaterial
+    from fem.mesh.structured import build_structured_hex8_box
+    from fem.rve import (RVERequest, StructuredHex8RVE, build_structured_hex8_periodic_constraint,
+                         initialize_rve_state, solve_rve_microequilibrium)  # fmt: skip
+    from fem.solvers.data import ArmijoSettings, NonlinearNewtonSettings
+
+    sys.path.insert(0, str(REPO))
+    from concrete_impact_b200.rve_builders import draw_spheres, solve_mixed_control_step, sphere_phase_map, uniaxial_path
+
+    update = MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10)
+    mortar = J2ViscoplasticMaterial("mortar", 2200.0, 25.0e9, 0.2, 20.0e6, 2.0e9, 1.0e-3, 20.0e6, 1.0)
+    aggregate = LinearElasticMaterial("aggregate", 2600.0, 50.0e9, 0.2)
+    newton = NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=False))
+    div = (8, 8, 8)
+    nodes, elements = build_structured_hex8_box((1.0, 1.0, 1.0), div)
+    phase = sphere_phase_map(div, draw_spheres(0))
+    phased = PhasedMaterialModel("mortar__aggregate", (RVEPhase("matrix", mortar), RVEPhase("inclusion", aggregate)),
+                                 np.repeat(phase, 8), 2360.0)  # fmt: skip
+    model = StructuredHex8RVE(nodes, elements, div, phased, build_structured_hex8_periodic_constraint(nodes, div),
+                              newton, element_phase_ids=phase, phase_names=("matrix", "inclusion"))  # fmt: skip
+
+    def solve(request, state):
+        return solve_rve_microequilibrium(model, RVERequest(np.asarray(request.macro_strain), request.time_step, update,
+                                                            MaterialResponseRequirements(tangent=True)), state)  # fmt: skip
+
+    times, exx = uniaxial_path(100)
+    state = initialize_rve_state(model)
+    guess = np.zeros(6)
+    strain, stress, outer = [], [], []
+    for step in range(1, steps + 1):
+        res = solve_mixed_control_step(solve, state, {0: float(exx[step])}, guess, float(times[step] - times[step - 1]),
+                                       update, stress_tolerance=1.0e-6 * 20.0e6)  # fmt: skip
+        state = res.response.state
+        guess = res.macro_strain
+        strain.append(res.macro_strain.copy())
+        stress.append(np.asarray(res.response.macro_stress))
+        outer.append(int(res.outer_iterations))
+    arrays = {"element_phase": phase.astype(np.uint8), "times": times[: steps + 1], "macro_strain": np.asarray(strain),
+              "macro_stress": np.asarray(stress)}  # fmt: skip
+    meta = {"kind": "mixed_control_path", "divisions": div, "layout_seed": 0, "steps": steps,
+            "outer_iterations": outer, "stress_tolerance": 1.0e-6 * 20.0e6,
+            "newton": [25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, False]}  # fmt: skip
+    return {"rve_path_uniaxial_8": (arrays, meta)}
 
 
 def make_rve_cases():
@@ -484,7 +611,7 @@ def make_rno_energy_cases(src: str):
     return {"rno_energy_c48": (arrays, meta)}
 
 
-GROUPS = ("j2", "rve", "newmark", "ogrid", "rno_energy")
+GROUPS = ("j2", "rve", "newmark", "ogrid", "rno_energy", "rve_batch", "rve_path")
 
 
 def main() -> None:
@@ -513,6 +640,10 @@ def main() -> None:
         cases.update(make_ogrid_cases())
     if "rno_energy" in groups:
         cases.update(make_rno_energy_cases(args.reference))
+    if "rve_batch" in groups:
+        cases.update(make_rve_batch_cases())
+    if "rve_path" in groups:
+        cases.update(make_rve_path_cases())
     path = HERE / "manifest.json"
     manifest = json.loads(path.read_text()) if path.exists() and args.only else {}
     for name, (arrays, meta) in cases.items():
