@@ -55,6 +55,8 @@ def parse_args() -> argparse.Namespace:
     parser.add_argument("--points", type=int, default=N_POINTS, help=argparse.SUPPRESS)
     parser.add_argument("--e2e-steps", type=int, default=3)
     parser.add_argument("--no-cpu-baseline", action="store_true", help=argparse.SUPPRESS)
+    # rve_batch: number of RVEs (256 is the workload; fewer for a small profiling case)
+    parser.add_argument("--rves", type=int, default=256, help=argparse.SUPPRESS)
     args = parser.parse_args()
     steps, warmup = WORKLOAD_DEFAULTS[args.workload]
     args.steps = steps if args.steps is None else args.steps

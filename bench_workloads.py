@@ -138,6 +138,13 @@ def run_rve_path(args: argparse.Namespace) -> None:
 
 PCG_TANGENT_BYTES_PER_GP = 8 * 4  # FP32 tangent parameters (n[6], f, c) of a plastic point
 PCG_VECTOR_BYTES_PER_ELEMENT = 10 * 3 * 8  # p gather, Ap write, x/r/p/dinv/Ap updates, FP64
+# Residual pass (rve_residual_kernel + gather), FP32 elements, per element of an active RVE:
+# 8 points x (committed state read: plastic strain 24 + eqps 8 + multiplier 8; trial write:
+# plastic strain 24 + eqps 8 + multiplier 8 + stress 24 + tangent data 32 + flag 1) + one
+# node's fluctuation 24 + element forces and diagonals 2 x 192 written + phase 1 = 1,505 B;
+# the gather reads the 384 B back and writes residual, inverse diagonal and trial w (72 B)
+# and reads w (24 B) = 480 B.
+RESIDUAL_BYTES_PER_ELEMENT_F32 = 8 * (40 + 97) + 24 + 384 + 1 + 480
 
 
 def _rve_batch_cpu(setup, sample_edges=(8, 12)) -> dict:
@@ -176,7 +183,7 @@ def run_rve_batch(args: argparse.Namespace) -> None:
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    setup = rve_batch_setup(256, 200)
+    setup = rve_batch_setup(getattr(args, "rves", 256), 200)
     forcing = os.environ.get("CIB_RVE_FORCING", "eisenstat_walker") or None
     with ClockSampler(local) as clocks:
         out = rve_batch_workload(setup, args.warmup, args.steps, forcing=forcing)
@@ -185,10 +192,14 @@ def run_rve_batch(args: argparse.Namespace) -> None:
     seconds = out["ms"] / 1e3
     value = out["gp_evaluations"] / seconds
     peak, kind = _peak()
+    bd = out["breakdown"]  # the steps whose kernels were timed one by one
     pcg_ms = out["kernel_ms"].get("pcg", 0.0)
-    pcg_bytes = out["pcg_element_iterations"] * (8 * PCG_TANGENT_BYTES_PER_GP * out["plastic_fraction"]
-                                                 + PCG_VECTOR_BYTES_PER_ELEMENT)  # fmt: skip
+    pcg_bytes = bd["pcg_element_iterations"] * (8 * PCG_TANGENT_BYTES_PER_GP * out["plastic_fraction"]
+                                                + PCG_VECTOR_BYTES_PER_ELEMENT)  # fmt: skip
     achieved = pcg_bytes / (pcg_ms / 1e3) / 1e9 if pcg_ms > 0 else None
+    res_ms = out["kernel_ms"].get("residual", 0.0)
+    res_bytes = bd["gp_evaluations"] / 8 * RESIDUAL_BYTES_PER_ELEMENT_F32
+    res_achieved = res_bytes / (res_ms / 1e3) / 1e9 if res_ms > 0 else None
     cpu = None
     if not args.no_cpu_baseline:
         c = _rve_batch_cpu(setup)
@@ -204,9 +215,24 @@ def run_rve_batch(args: argparse.Namespace) -> None:
                   "accepted_rve_steps_per_s": rve_steps_s, "elements": out["elements"],
                   "gauss_points": out["gauss_points"], "newton_max": out["newton_max"], "pcg_max": out["pcg_max"],
                   "pcg_total": out["pcg_total"], "plastic_fraction": out["plastic_fraction"],
-                  "pcg_cluster": out["pcg_cluster"], "pcg_cluster_tuning_ms": (out["tuning"] or {}).get("ms"),
+                  "pcg_cluster": out["pcg_cluster"], "pcg_shape": out["pcg_shape"],
+                  "pcg_tuning": {"ms": (out["tuning"] or {}).get("ms"), "cached": (out["tuning"] or {}).get("cached"),
+                                 "key": "cluster size / launch shape (0: 256 threads default cap, 1: 128 threads, "
+                                        "2: 512 threads, 3: 256 threads other register cap)"},
                   "newton_forcing": out["forcing"],
+                  "newton_control": ("device: one CUDA graph per step (conditional while loop over the Newton "
+                                     "iterations; residual, gather x2, check, PCG, update, axpy kernels per iteration)"
+                                     if out["device_control"] else "host loop (two read-backs per Newton iteration)"),
+                  "graph_launches_per_step": 1 if out["device_control"] else 0,
+                  "host_syncs_per_step": 2 if out["device_control"] else None,
+                  "graph_loop_iterations": out["graph_loops"],
                   "kernel_ms": out["kernel_ms"], "kernel_launches": out["kernel_launches"],
+                  "kernel_breakdown_steps": bd["steps"],
+                  "residual_roofline": {"bound": "hbm", "achieved": res_achieved, "peak": peak, "unit": "GB/s",
+                                        "frac": None if res_achieved is None else res_achieved / peak,
+                                        "kernel": "rve_residual_kernel<float> + rve_gather_nodes/norms_kernel",
+                                        "bytes_per_element": RESIDUAL_BYTES_PER_ELEMENT_F32,
+                                        "algorithmic_bytes": res_bytes},
                   "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                "frac": None if achieved is None else achieved / peak, "traffic": None,
                                "peak_kind": kind, "kernel": "rve_pcg_cluster_kernel<float> (rve_pcg_kernel at cluster 1)",

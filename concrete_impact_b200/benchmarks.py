@@ -145,59 +145,85 @@ def rve_batch_setup(n_rve: int = 256, steps: int = 200, edges=EDGES, base_seed: 
 
 
 def rve_batch_workload(setup: RVEBatchSetup, warmup: int, timed: int, precision: int = 32, tune: bool = True,
-                       forcing: str | None = "eisenstat_walker") -> dict:  # fmt: skip
+                       forcing: str | None = "eisenstat_walker", device_control: bool = True,
+                       breakdown_steps: int = 2) -> dict:  # fmt: skip
     """Advance every RVE of the batch ``warmup`` path steps untimed, then ``timed`` steps
     timed; one step = one batched Newton solve (+ homogenisation and commit) per time index.
     Each step copies its macro strains and time steps from pinned host memory and reads the
     homogenised stresses back (the caller's view of the batched API).  With ``tune`` the PCG
     cluster size is measured (``tune_pcg_cluster``) on the first timed step's system before
     the timed region.  ``forcing`` selects the inexact-Newton PCG tolerance
-    (LinearSolverOptions.forcing)."""
-    batch = RVEBatch(setup.models, precision=precision, linear_solver=LinearSolverOptions(forcing=forcing))
+    (LinearSolverOptions.forcing).  With ``device_control`` every step's Newton solve is one
+    CUDA graph launch (decisions on the device); ``breakdown_steps`` further steps then run
+    through the host-driven loop with CUDA events around its residual and PCG launches, for
+    the per-kernel times (the graph hides them)."""
+    batch = RVEBatch(setup.models, precision=precision, linear_solver=LinearSolverOptions(forcing=forcing),
+                     device_control=device_control)  # fmt: skip
     dev = batch.device
     strain_h = torch.as_tensor(setup.strains).pin_memory()
     dt_h = torch.as_tensor(np.diff(setup.times, axis=1)).pin_memory()
     stress_h = torch.empty((batch.nrve, 6), dtype=torch.float64).pin_memory()
     newton = setup.models[0].newton_settings
     gp = 8 * batch.elem_counts
-    counts = {"gp_evaluations": 0, "newton_max": 0, "pcg_max": 0, "pcg_total": 0, "pcg_element_iterations": 0}
+    keys = ("gp_evaluations", "newton_max", "pcg_max", "pcg_total", "pcg_element_iterations", "graph_loops")
+    counts = dict.fromkeys(keys, 0)
+    breakdown = dict.fromkeys(keys, 0)
     vol = torch.as_tensor(batch.volumes, device=dev)[:, None]
     timers: dict = {}
 
-    def step(t: int, record: bool) -> None:
+    def step(t: int, tally: dict | None, step_timers: dict | None = None) -> None:
         batch.macro.copy_(strain_h[:, t], non_blocking=True)
         batch.dt.copy_(dt_h[:, t - 1], non_blocking=True)
-        res = solve_batch_step(batch, newton, UPDATE_SETTINGS, False, timers=timers if record else None)
+        res = solve_batch_step(batch, newton, UPDATE_SETTINGS, False, timers=step_timers)
         batch.response(batch.batch_struct(UPDATE_SETTINGS), batch.w, None, None)
         stress_h.copy_(batch.sums[:, RS_SIGMA : RS_SIGMA + 6] / vol)
         batch.commit()
-        if record:
+        if tally is not None:
             passes = res.newton_iterations + 1 + res.armijo_backtracks
-            counts["gp_evaluations"] += int((passes * gp).sum())
-            counts["newton_max"] = max(counts["newton_max"], int(res.newton_iterations.max()))
-            counts["pcg_max"] = max(counts["pcg_max"], int(res.pcg_iterations.max()))
-            counts["pcg_total"] += int(res.pcg_iterations.sum())
-            counts["pcg_element_iterations"] += int((res.pcg_iterations * batch.elem_counts).sum())
+            tally["gp_evaluations"] += int((passes * gp).sum())
+            tally["newton_max"] = max(tally["newton_max"], int(res.newton_iterations.max()))
+            tally["pcg_max"] = max(tally["pcg_max"], int(res.pcg_iterations.max()))
+            tally["pcg_total"] += int(res.pcg_iterations.sum())
+            tally["pcg_element_iterations"] += int((res.pcg_iterations * batch.elem_counts).sum())
+            if batch.device_control:
+                tally["graph_loops"] += batch.last_graph_iterations
 
     for t in range(1, warmup + 1):
-        step(t, False)
+        step(t, None)
     tuning = None
     if tune:
         batch.macro.copy_(strain_h[:, warmup + 1])
         batch.dt.copy_(dt_h[:, warmup])
-        tuning = tune_pcg_cluster(batch, UPDATE_SETTINGS)
+        tuning = tune_pcg_cluster(batch, UPDATE_SETTINGS, persist=False)  # measured in every run
+    if device_control:  # build the step's graph outside the timed region
+        batch.newton_graph(newton, UPDATE_SETTINGS)
     calls0 = _native.LAUNCHED[0]
-    ms = _elapsed_ms(lambda: [step(t, True) for t in range(warmup + 1, warmup + timed + 1)])
+    last = warmup + timed
+    ms = _elapsed_ms(lambda: [step(t, counts, None if device_control else timers)
+                              for t in range(warmup + 1, last + 1)])  # fmt: skip
     launched = _native.LAUNCHED[0] - calls0
+    if device_control:  # a graph launch runs init + 7 kernels per loop + finish
+        launched += 7 * counts["graph_loops"] + timed
+    breakdown_range = range(warmup + 1, last + 1)
+    if device_control:
+        # per-kernel times from further steps through the host-driven loop (the same kernels
+        # and decisions, with CUDA events around its residual and PCG launches), untimed
+        batch.device_control = False
+        breakdown_range = range(last + 1, min(last + breakdown_steps, setup.strains.shape[1] - 1) + 1)
+        for t in breakdown_range:
+            step(t, breakdown, timers)
+        batch.device_control = True
+    else:
+        breakdown = dict(counts)
     kernel_ms = {k: float(sum(a.elapsed_time(b) for a, b in v)) for k, v in timers.items()}
     launches = {k: len(v) for k, v in timers.items()}
     plastic = float(batch.tflag.float().mean().item())
     return {"ms": ms, "rve_steps": batch.nrve * timed, "gauss_points": int(gp.sum()), "elements": int(batch.nelem),
             "stress_last": stress_h.numpy().copy(), "kernel_ms": kernel_ms, "kernel_launches": launches,
             "plastic_fraction": plastic, "h2d_bytes_per_step": int(batch.nrve * 7 * 8),
-            "d2h_bytes_per_step": int(batch.nrve * 6 * 8), "pcg_cluster": int(batch.cluster), "tuning": tuning,
-            "forcing": forcing,
-            "launches": launched,
+            "d2h_bytes_per_step": int(batch.nrve * 6 * 8), "pcg_cluster": int(batch.cluster), "pcg_shape": int(batch.pcg_shape), "tuning": tuning,
+            "forcing": forcing, "device_control": device_control,
+            "launches": launched, "breakdown": {"steps": len(breakdown_range), **breakdown},
             **counts}  # fmt: skip
 
 

@@ -842,8 +842,30 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NV], double* scratch, do
   for (int k = 0; k < NV; ++k) v[k] = t[k];
 }
 
+// Launch shapes of the cluster PCG (threads per CTA, resident CTAs per SM -> register cap),
+// chosen per batch by the tuner: 0 is the default, 1-3 trade threads for registers.
+template <typename T, int SHAPE>
+struct PcgShape;
 template <typename T>
-__global__ void __launch_bounds__(RVE_THREADS, sizeof(T) == 4 ? 2 : 1) rve_pcg_cluster_kernel(const RvePcgArgs<T> a) {
+struct PcgShape<T, 0> {
+  static constexpr int threads = 256, min_blocks = sizeof(T) == 4 ? 2 : 1;
+};
+template <typename T>
+struct PcgShape<T, 1> {
+  static constexpr int threads = 128, min_blocks = sizeof(T) == 4 ? 4 : 2;
+};
+template <typename T>
+struct PcgShape<T, 2> {
+  static constexpr int threads = 512, min_blocks = 1;
+};
+template <typename T>
+struct PcgShape<T, 3> {
+  static constexpr int threads = 256, min_blocks = sizeof(T) == 4 ? 1 : 2;
+};
+
+template <typename T, int SHAPE>
+__global__ void __launch_bounds__(PcgShape<T, SHAPE>::threads, PcgShape<T, SHAPE>::min_blocks)
+    rve_pcg_cluster_kernel(const RvePcgArgs<T> a) {
   extern __shared__ double smem_dyn[];  // the layer buffers of apply_tangent_slab
   unsigned char* smem = reinterpret_cast<unsigned char*>(smem_dyn);
   __shared__ double scratch[64];
@@ -1358,17 +1380,14 @@ int launch_rve_pcg(const RvePcgArgs<T>& a, int nsys, int max_nxy, cudaStream_t s
   return check_launch();
 }
 
-template <typename T>
-int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cluster, cudaStream_t st) {
-  if (cluster == 1) return launch_rve_pcg<T>(a, nsys, max_nxy, st);
-  if (cluster != 2 && cluster != 4 && cluster != 8) return CIB_EINVAL;
-  const size_t smem = (size_t)max_nxy * (24 * sizeof(T) + 12 * sizeof(double));
-  if (smem > 200 * 1024) return CIB_ERANGE;
-  const int rc = allow_dynamic_smem(reinterpret_cast<const void*>(rve_pcg_cluster_kernel<T>), 200 * 1024);
+template <typename T, int SHAPE>
+int launch_rve_pcg_cluster_shape(const RvePcgArgs<T>& a, int nsys, int cluster, size_t smem, cudaStream_t st) {
+  const void* fn = reinterpret_cast<const void*>(rve_pcg_cluster_kernel<T, SHAPE>);
+  const int rc = allow_dynamic_smem(fn, 200 * 1024);
   if (rc != CIB_OK) return rc;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)nsys * (unsigned)cluster, 1, 1);
-  cfg.blockDim = dim3(RVE_THREADS, 1, 1);
+  cfg.blockDim = dim3(PcgShape<T, SHAPE>::threads, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -1378,8 +1397,26 @@ int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cl
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, rve_pcg_cluster_kernel<T>, a);
+  cudaLaunchKernelEx(&cfg, rve_pcg_cluster_kernel<T, SHAPE>, a);
   return check_launch();
+}
+
+// cluster: the CTAs per system (1, 2, 4 or 8) in bits 0-3 and the launch shape (0-3, see
+// PcgShape) in bits 4-7; cluster size 1 is the one-CTA kernel, whatever the shape.
+template <typename T>
+int launch_rve_pcg_cluster(const RvePcgArgs<T>& a, int nsys, int max_nxy, int cluster, cudaStream_t st) {
+  const int c = cluster & 15, shape = (cluster >> 4) & 15;
+  if ((cluster >> 8) != 0 || shape > 3) return CIB_EINVAL;
+  if (c == 1) return launch_rve_pcg<T>(a, nsys, max_nxy, st);
+  if (c != 2 && c != 4 && c != 8) return CIB_EINVAL;
+  const size_t smem = (size_t)max_nxy * (24 * sizeof(T) + 12 * sizeof(double));
+  if (smem > 200 * 1024) return CIB_ERANGE;
+  switch (shape) {
+    case 1: return launch_rve_pcg_cluster_shape<T, 1>(a, nsys, c, smem, st);
+    case 2: return launch_rve_pcg_cluster_shape<T, 2>(a, nsys, c, smem, st);
+    case 3: return launch_rve_pcg_cluster_shape<T, 3>(a, nsys, c, smem, st);
+    default: return launch_rve_pcg_cluster_shape<T, 0>(a, nsys, c, smem, st);
+  }
 }
 
 template <typename T>

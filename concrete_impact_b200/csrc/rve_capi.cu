@@ -7,6 +7,12 @@
 namespace cib {
 namespace {
 
+// CTAs per system (1, 2, 4, 8) in bits 0-3, launch shape (0-3) in bits 4-7.
+bool pcg_cluster_ok(int32_t cluster) {
+  const int c = cluster & 15;
+  return cluster >= 0 && (cluster >> 8) == 0 && ((cluster >> 4) & 15) <= 3 && (c == 1 || c == 2 || c == 4 || c == 8);
+}
+
 bool batch_ok(const cib_rve_batch* b) {
   return b && b->nrve >= 0 && b->nphase >= 1 && b->nphase <= RVE_MAX_PHASES && b->nelem >= 0 && b->desc &&
          b->phase && (b->precision == 32 || b->precision == 64);
@@ -126,7 +132,7 @@ extern "C" int cib_rve_pcg_cluster(const cib_rve_batch* batch, int32_t nsys, con
                                    double* xnorm, void* stream) {
   if (!batch_ok(batch) || nsys < 0 || !sys_rve || !sys_off || !b || !dinv || !x || !r || !p || !Ap || !status ||
       !iterations || !rel_residual || !xnorm || maxit < 0 || !batch->tparam || !batch->tflag || batch->max_nxy <= 0 ||
-      (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8))
+      !pcg_cluster_ok(cluster))
     return CIB_EINVAL;
   if (nsys == 0) return CIB_OK;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);

@@ -409,7 +409,9 @@ extern "C" int cib_rve_newton_graph_create(const cib_rve_batch* batch, const cib
       !batch->vpm || !batch->stress || !batch->tparam || !batch->tflag || !batch->fe || !batch->de)
     return CIB_EINVAL;
   if (!s || s->max_iterations < 0 || s->pcg_maxit < 0 ||
-      (s->cluster != 1 && s->cluster != 2 && s->cluster != 4 && s->cluster != 8) || !s->time_step || !s->macro ||
+      s->cluster < 0 || (s->cluster >> 8) != 0 || ((s->cluster >> 4) & 15) > 3 ||
+      ((s->cluster & 15) != 1 && (s->cluster & 15) != 2 && (s->cluster & 15) != 4 && (s->cluster & 15) != 8) ||
+      !s->time_step || !s->macro ||
       !s->w_n || !s->w || !s->w_out || !s->x || !s->r || !s->p || !s->Ap || !s->residual || !s->dinv || !s->rnorm2 ||
       !s->wnorm2 || !s->class_max || !s->alpha || !s->active || !s->fail || !s->sys_rve || !s->sys_off ||
       !s->pcg_status || !s->pcg_iterations || !s->pcg_rel_residual || !s->pcg_xnorm || !s->iwork || !s->dwork)

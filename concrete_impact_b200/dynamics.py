@@ -566,14 +566,20 @@ _ACTIVITY = ("incremental_work_density", "viscoplastic_active", "yield_activatio
 class _Recorder:
     """Histories of the accepted states (src/fem/dynamics/material.py:732-927)."""
 
-    def __init__(self, ops: MacroOperators, load_function: LoadFunction, record_fields: bool) -> None:
+    def __init__(self, ops: MacroOperators, load_function: LoadFunction, record_fields: bool,
+                 lumped_mass: torch.Tensor | None = None, record_state: bool = False) -> None:  # fmt: skip
         self.ops, self.load, self.fields = ops, load_function, record_fields
+        self.lumped = lumped_mass  # explicit runs: kinetic energy with the lumped mass
+        self.record_state = record_state
         self.rows: list[dict[str, Any]] = []
         self.accepted = 0
 
     def record(self, state: _StepState, interval: _Interval | None, rejected: tuple[str, ...] = ()) -> None:
         ops, asm = self.ops, state.assembly
-        kinetic = 0.5 * float(torch.dot(state.velocity, ops.spmv(ops.mass, state.velocity)))
+        if self.lumped is not None:
+            kinetic = 0.5 * float(torch.sum(self.lumped * state.velocity**2))
+        else:
+            kinetic = 0.5 * float(torch.dot(state.velocity, ops.spmv(ops.mass, state.velocity)))
         row: dict[str, Any] = {
             "time": state.time, "kinetic": kinetic, "free": ops.integrate(asm.free_energy),
             "dissipation": interval.dissipation_increment if interval else 0.0,
@@ -594,6 +600,9 @@ class _Recorder:
         if interval is not None:
             self.accepted += 1
         row["fields"] = self._fields(state) if self.fields else None
+        if self.record_state:
+            row["state"] = {k: (v.cpu().numpy() if isinstance(v, torch.Tensor) else np.asarray(v)).copy()
+                            for k, v in state.material_state.variables.items()}  # fmt: skip
         self.last = state
         self.rows.append(row)
 
@@ -615,7 +624,7 @@ class _Recorder:
             "psi": host(asm.free_energy), "diss": host(asm.dissipation),
         }  # fmt: skip
 
-    def solution(self, final: _StepState, solve_time: float) -> MaterialDynamicSolution:
+    def solution(self, final: _StepState, solve_time: float, integrator: dict | None = None) -> MaterialDynamicSolution:
         rows = self.rows
         steps = len(rows)
         col = lambda k, default=0.0: np.asarray([r.get(k, default) for r in rows], dtype=np.float64)  # noqa: E731
@@ -646,6 +655,133 @@ class _Recorder:
             rejected_step_counts=np.asarray([len(r["rejected"]) for r in rows], dtype=np.int64),
             armijo_backtracks=col("armijo").astype(np.int64),
             rejected_reasons=tuple(r["rejected"] for r in rows), material_diagnostics=material_diagnostics,
-            integrator_diagnostics={"linear_iterations": np.asarray([self.ops.linear_iterations], dtype=np.int64)},
+            integrator_diagnostics=(integrator if integrator is not None else
+                                    {"linear_iterations": np.asarray([self.ops.linear_iterations], dtype=np.int64)}),
             final_state=final_state, solve_time=solve_time,
+            material_state_history=({k: np.stack([r["state"][k] for r in rows]) for k in rows[0]["state"]}
+                                    if self.record_state else None),
         )  # fmt: skip
+
+
+# --------------------------------------------------------------------------------------
+# Explicit velocity-Verlet material dynamics (src/fem/dynamics/material.py:89-297) and its
+# CFL check (src/fem/dynamics/stability.py:34-100).
+
+# Hex8 element edges in the reference's node order (stability.py EDGE_NODE_TABLE["hex8"]).
+HEX8_EDGES = ((0, 1), (0, 2), (1, 3), (2, 3), (4, 5), (4, 6), (5, 7), (6, 7), (0, 4), (1, 5), (2, 6), (3, 7))
+
+
+@dataclass(frozen=True)
+class StabilityReport:
+    """Explicit CFL data: smallest element edge, material wave-speed bound, stable step."""
+
+    minimum_length: float
+    maximum_wave_speed: float
+    stable_time_step: float
+    requested_time_step: float
+
+
+def compute_explicit_stability_report(mesh, time_settings: TimeIntegrationSettings) -> StabilityReport:
+    """cfl_safety_factor x the smallest Hex8 edge / the material's maximum wave speed."""
+    nodes, elements, material = _mesh_fields(mesh)
+    edges = np.asarray(HEX8_EDGES)
+    vectors = nodes[elements[:, edges[:, 1]]] - nodes[elements[:, edges[:, 0]]]
+    minimum_length = float(np.sqrt(np.min(np.einsum("eki,eki->ek", vectors, vectors))))
+    speed = float(material.maximum_wave_speed)
+    return StabilityReport(minimum_length, speed, time_settings.cfl_safety_factor * minimum_length / speed,
+                           time_settings.time_step)  # fmt: skip
+
+
+def check_explicit_stability(mesh, time_settings: TimeIntegrationSettings) -> StabilityReport:
+    """Raise ValueError when the requested explicit step exceeds the CFL bound."""
+    report = compute_explicit_stability_report(mesh, time_settings)
+    if time_settings.time_step > report.stable_time_step:
+        raise ValueError("Explicit time step violates the CFL stability bound: "
+                         f"dt={time_settings.time_step:.6e}, dt_crit={report.stable_time_step:.6e}.")  # fmt: skip
+    return report
+
+
+def solve_material_explicit(
+    mesh,
+    time_settings: TimeIntegrationSettings,
+    initial_displacement,
+    initial_velocity,
+    dirichlet: DirichletDofSet,
+    load_function: LoadFunction,
+    kinematics: str,
+    update_settings: MaterialUpdateSettings,
+    progress_callback: Callable[[dict[str, Any]], None] | None = None,
+    residual_corrector=None,
+    correction_controls=None,
+    record_material_state_history: bool = False,
+    record_fields: bool = True,
+    operators: MacroOperators | None = None,
+) -> MaterialDynamicSolution:
+    """Material dynamics by explicit velocity Verlet with the row-sum lumped mass
+    (src/fem/dynamics/material.py:89-297), same arguments and histories as the reference.
+
+    Every step runs on the device: the Verlet predictor (``cib_verlet_predict``), Hex8
+    strains, the material update at every integration point (J2 kernels, or one device
+    batch of periodic RVE solves for ``RVEHomogenizedMaterial``: explicit FE^2), internal
+    force, and the corrector with the next load (``cib_verlet_correct``).  The lumped mass
+    is the row sum of the consistent mass, assembled on the device.  The reference's
+    optional velocity-Verlet residual corrector (a surrogate hook) is not supported.
+    ``record_fields`` False keeps the per-DOF and per-point histories of the final state
+    only (scalar histories are always complete)."""
+    if np.any(np.asarray(dirichlet.values) != 0.0):
+        raise ValueError("Material dynamics currently requires homogeneous Dirichlet values.")
+    stability = check_explicit_stability(mesh, time_settings)
+    if residual_corrector is None and correction_controls is not None:
+        raise ValueError("Correction controls require an enabled residual corrector.")
+    if residual_corrector is not None:
+        raise NotImplementedError("The velocity-Verlet residual corrector is not supported on the GPU path.")
+    if kinematics != "three_dimensional":
+        raise ValueError("The GPU Hex8 material dynamics supports kinematics='three_dimensional' only.")
+    start_time = perf_counter()
+    nodes, elements, material = _mesh_fields(mesh)
+    ops = operators or MacroOperators(nodes, elements, material.density, dirichlet.dofs)
+    lib, dev = ops.lib, ops.device
+    dt = float(time_settings.time_step)
+    steps = int(time_settings.num_steps)
+    lumped = ops.spmv(ops.mass, torch.ones(ops.n, dtype=torch.float64, device=dev))
+    fixed = (1 - ops.free).to(torch.uint8).contiguous()
+    u = ops.vector(initial_displacement).clone()
+    v = ops.vector(initial_velocity).clone()
+    u[ops.fixed] = 0.0
+    v[ops.fixed] = 0.0
+    state = initialize_hex8_material_state(material, int(elements.shape[0]))
+    assembly = assemble_hex8_material_response_cached(nodes, elements, material, state, u, u, dt, update_settings,
+                                                      ops.cache, False)  # fmt: skip
+    external = ops.vector(load_function(0.0))
+    a = (external - assembly.internal_force) / lumped
+    a[ops.fixed] = 0.0
+    current = _StepState(0.0, u, v, a, assembly.state, assembly)
+    rec = _Recorder(ops, load_function, record_fields, lumped_mass=lumped, record_state=record_material_state_history)
+    rec.record(current, None)
+    stream = _native.stream_ptr
+    for step in range(steps):
+        t1 = (step + 1) * dt
+        u1 = torch.empty_like(u)
+        _native.check(lib.cib_verlet_predict(ops.n, current.displacement.data_ptr(), current.velocity.data_ptr(),
+                                             current.acceleration.data_ptr(), fixed.data_ptr(), dt, u1.data_ptr(),
+                                             stream()), "cib_verlet_predict")  # fmt: skip
+        asm = assemble_hex8_material_response_cached(nodes, elements, material, current.material_state, u1,
+                                                     current.displacement, dt, update_settings, ops.cache, False)  # fmt: skip
+        external1 = ops.vector(load_function(t1))
+        a1, v1 = torch.empty_like(u), torch.empty_like(u)
+        _native.check(lib.cib_verlet_correct(ops.n, external1.data_ptr(), 1.0, asm.internal_force.data_ptr(),
+                                             lumped.data_ptr(), fixed.data_ptr(), dt, current.acceleration.data_ptr(),
+                                             current.velocity.data_ptr(), a1.data_ptr(), v1.data_ptr(), stream()),
+                      "cib_verlet_correct")  # fmt: skip
+        dissipation = dt * ops.integrate(asm.dissipation)
+        work = float(0.5 * torch.dot(external + external1, u1 - current.displacement))
+        current = _StepState(t1, u1, v1, a1, asm.state, asm)
+        rec.record(current, _Interval(current, dissipation, work, 0, 0))
+        external = external1
+        if progress_callback is not None:
+            progress_callback({"stage": "material_dynamics", "scheme": "explicit", "accepted_step": step + 1,
+                               "nominal_total_steps": steps, "physical_time": t1, "final_time": steps * dt,
+                               "newton_iterations": 0, "armijo_backtracks": 0,
+                               "elapsed_seconds": perf_counter() - start_time})  # fmt: skip
+    del stability  # checked above; the reference returns no integrator diagnostics without a corrector
+    return rec.solution(current, perf_counter() - start_time, integrator={})

@@ -24,9 +24,12 @@ or a ``PhasedMaterialModel`` of those, for one RVE or a batch of RVEs of differe
 from __future__ import annotations
 
 import ctypes
+import json
 import math
+import os
 from collections.abc import Callable, Iterator
 from dataclasses import dataclass, field
+from pathlib import Path
 from time import perf_counter
 from typing import Any, Literal
 
@@ -447,6 +450,7 @@ class RVEBatch:
         c = self.linear.cluster
         self.cluster = auto_pcg_cluster(self) if c == "auto" else self.check_cluster(int(c))
         self._batch_struct = None
+        self.pcg_shape = 0
         self.device_control = bool(device_control)
         self.live_mask = torch.ones(self.nrve, dtype=torch.int32, device=dev)
         self._graphs: dict = {}
@@ -492,6 +496,11 @@ class RVEBatch:
         )  # fmt: skip
         _native.check(code, "cib_rve_gather")
 
+    def pcg_launch(self) -> int:
+        """The ``cluster`` argument of cib_rve_pcg_cluster: CTAs per system in bits 0-3, the
+        launch shape (threads per CTA / register cap) in bits 4-7."""
+        return int(self.cluster) | (int(self.pcg_shape) << 4)
+
     def check_cluster(self, cluster: int) -> int:
         if cluster not in (1, 2, 4, 8):
             raise ValueError("the PCG cluster size must be 1, 2, 4 or 8")
@@ -505,7 +514,7 @@ class RVEBatch:
             ctypes.byref(b), nsys, sys_rve.data_ptr(), sys_off.data_ptr(), self.active.data_ptr(), rhs.data_ptr(),
             self.dinv.data_ptr(), x.data_ptr(), r.data_ptr(), p.data_ptr(), Ap.data_ptr(),
             float(self.rtol if rtol is None else rtol),
-            int(self.linear.max_iterations), int(self.cluster), status.data_ptr(), iters.data_ptr(), rel.data_ptr(),
+            int(self.linear.max_iterations), self.pcg_launch(), status.data_ptr(), iters.data_ptr(), rel.data_ptr(),
             xnorm.data_ptr(), _native.stream_ptr(),
         )  # fmt: skip
         _native.check(code, "cib_rve_pcg_cluster")
@@ -551,7 +560,7 @@ class RVEBatch:
     def newton_graph(self, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings) -> "_NewtonGraph":
         """The device-controlled Newton graph for these settings (built once, then reused;
         the PCG cluster size and tolerances in force are part of the key)."""
-        key = (tuple(_newton_key(newton)), repr(update_settings), self.cluster, float(self.rtol),
+        key = (tuple(_newton_key(newton)), repr(update_settings), self.pcg_launch(), float(self.rtol),
                int(self.linear.max_iterations), self.linear.forcing)  # fmt: skip
         graph = self._graphs.get(key)
         if graph is None:
@@ -616,7 +625,7 @@ class _NewtonGraph:
         s.increment_relative_tolerance = float(newton.increment_relative_tolerance)
         s.pcg_rtol = float(batch.rtol)
         s.pcg_maxit = int(batch.linear.max_iterations)
-        s.cluster = int(batch.cluster)
+        s.cluster = batch.pcg_launch()
         for name, tensor in (("time_step", batch.dt), ("macro", batch.macro), ("w_n", batch.w_n), ("w", batch.w),
                              ("w_out", batch.w_out), ("x", batch.x), ("r", batch.r), ("p", batch.p), ("Ap", batch.Ap),
                              ("residual", batch.res), ("dinv", batch.dinv), ("rnorm2", batch.rnorm2),
@@ -656,6 +665,7 @@ def _solve_batch_step_graph(batch: RVEBatch, newton: NonlinearNewtonSettings, up
         batch.live_mask.copy_(torch.as_tensor(np.asarray(live_mask, dtype=np.int32), device=batch.device))
     graph.launch()
     iw = graph.iwork.cpu().numpy()
+    batch.last_graph_iterations = int(iw[0])  # loop bodies run (for launch accounting)
     dw = graph.dwork.cpu().numpy()
     its, pcg = iw[_CTL : _CTL + R].astype(np.int64), iw[_CTL + R : _CTL + 2 * R].astype(np.int64)
     rnorm, tol = dw[_CTL : _CTL + R], dw[_CTL + R : _CTL + 2 * R]
@@ -812,30 +822,80 @@ def auto_pcg_cluster(batch: RVEBatch) -> int:
     return c
 
 
-def tune_pcg_cluster(batch: RVEBatch, update_settings: MaterialUpdateSettings, candidates=(1, 2, 4, 8)) -> dict:
+PCG_SHAPES = {0: "256 threads, default register cap", 1: "128 threads, 4 (FP64: 2) CTAs per SM",
+              2: "512 threads, 1 CTA per SM", 3: "256 threads, the other register cap (FP32: 1, FP64: 2 CTAs per SM)"}
+
+
+def _tuning_path() -> Path:
+    base = os.environ.get("CIB_TUNING_CACHE")
+    if base:
+        return Path(base)
+    return Path(os.environ.get("XDG_CACHE_HOME", Path.home() / ".cache")) / "cib200" / "pcg_tuning.json"
+
+
+def _edge_mix_key(batch: RVEBatch) -> str:
+    """The tuning key of a batch: precision, GPU name and the multiset of RVE divisions."""
+    mix: dict[str, int] = {}
+    for m in batch.models:
+        d = "x".join(str(int(v)) for v in m.divisions)
+        mix[d] = mix.get(d, 0) + 1
+    name = torch.cuda.get_device_name(batch.device)
+    return f"f{batch.precision}|{name}|" + ",".join(f"{k}:{mix[k]}" for k in sorted(mix))
+
+
+def tune_pcg_cluster(batch: RVEBatch, update_settings: MaterialUpdateSettings, candidates=(1, 2, 4, 8),
+                     shapes=(0, 1, 2, 3), persist: bool = True) -> dict:  # fmt: skip
     """Time one PCG solve of the batch's current Newton system (a residual pass at the
-    committed fluctuation) for each admissible cluster size and keep the fastest.  The
-    solves write only work vectors; the batch's state is unchanged.  Returns
-    {"cluster": best, "ms": {size: milliseconds}}."""
+    committed fluctuation) for every admissible cluster size x launch shape (threads per
+    CTA and register cap, ``PCG_SHAPES``; shapes apply to cluster sizes above 1) and keep
+    the fastest.  The solves write only work vectors; the batch's state is unchanged.
+    With ``persist`` the choice is stored per edge mix (precision, GPU, RVE divisions) in
+    a JSON file (``$CIB_TUNING_CACHE``, else ``~/.cache/cib200/pcg_tuning.json``) and a
+    later call for the same mix takes it from there without timing.  Returns
+    {"cluster": c, "shape": s, "ms": {"c/s": milliseconds}, "cached": bool, "key": key}."""
+    key = _edge_mix_key(batch)
+    path = _tuning_path()
+    table = {}
+    if persist and path.exists():
+        try:
+            table = json.loads(path.read_text())
+        except ValueError:
+            table = {}
+    hit = table.get(key)
+    if persist and hit and hit["cluster"] in candidates and hit["cluster"] <= batch.min_nz and hit["shape"] in shapes:
+        batch.cluster, batch.pcg_shape = int(hit["cluster"]), int(hit["shape"])
+        return {"cluster": batch.cluster, "shape": batch.pcg_shape, "ms": hit.get("ms", {}), "cached": True, "key": key}
     b = batch.batch_struct(update_settings)
-    saved = batch.cluster
+    saved = (batch.cluster, batch.pcg_shape)
     batch.w.copy_(batch.w_n)
     batch.residual(b, batch.w, None, None)
-    timings = {}
+    timings: dict[str, float] = {}
     for c in candidates:
         if c > batch.min_nz:
             continue
-        batch.cluster = c
-        for rep in range(2):  # the first run also sets the launch attributes
-            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            start.record()
-            batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, batch.nrve, batch.sys_rve, batch.sys_off,
-                      batch.pcg_status, batch.pcg_iters, batch.pcg_rel, batch.pcg_xnorm)  # fmt: skip
-            end.record()
-            torch.cuda.synchronize()
-        timings[c] = start.elapsed_time(end)
-    batch.cluster = min(timings, key=timings.get) if timings else saved
-    return {"cluster": batch.cluster, "ms": timings}
+        for shape in (shapes if c > 1 else (0,)):
+            batch.cluster, batch.pcg_shape = c, shape
+            for rep in range(2):  # the first run also sets the launch attributes
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record()
+                batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, batch.nrve, batch.sys_rve, batch.sys_off,
+                          batch.pcg_status, batch.pcg_iters, batch.pcg_rel, batch.pcg_xnorm)  # fmt: skip
+                end.record()
+                torch.cuda.synchronize()
+            timings[f"{c}/{shape}"] = start.elapsed_time(end)
+    if timings:
+        best = min(timings, key=timings.get)
+        batch.cluster, batch.pcg_shape = (int(v) for v in best.split("/"))
+    else:
+        batch.cluster, batch.pcg_shape = saved
+    if persist and timings:
+        table[key] = {"cluster": batch.cluster, "shape": batch.pcg_shape, "ms": timings}
+        try:
+            path.parent.mkdir(parents=True, exist_ok=True)
+            path.write_text(json.dumps(table, indent=1, sort_keys=True))
+        except OSError:
+            pass  # a read-only cache location only loses the persistence
+    return {"cluster": batch.cluster, "shape": batch.pcg_shape, "ms": timings, "cached": False, "key": key}
 
 
 def _timed(timers: dict | None, key: str, fn) -> None:

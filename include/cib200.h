@@ -293,8 +293,12 @@ int cib_rve_pcg(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve
  * each CTA owns a slab of z node layers, slab boundaries are exchanged and the dot
  * products combined through distributed shared memory (fixed rank order, so results are
  * reproducible for a given cluster size).  Every RVE needs nz >= cluster (else that
- * system's status is 3); cluster 1 is cib_rve_pcg.  Same reference interface as
- * cib_rve_pcg (Tᵀ K T + spsolve, src/fem/rve/solver.py:143-144). */
+ * system's status is 3); cluster 1 is cib_rve_pcg.  Bits 4-7 of `cluster` select the launch
+ * shape of the cluster kernel (threads per CTA / CTAs per SM, which caps the registers):
+ * 0 the default (256 / 2 in FP32, 256 / 1 in FP64), 1 (128 / 4 FP32, 128 / 2 FP64),
+ * 2 (512 / 1), 3 (256 / 1 FP32, 256 / 2 FP64); results do not depend on the shape beyond
+ * rounding of the CTA sums.  Same reference interface as cib_rve_pcg (Tᵀ K T + spsolve,
+ * src/fem/rve/solver.py:143-144). */
 int cib_rve_pcg_cluster(const cib_rve_batch* batch, int32_t nsys, const int32_t* sys_rve, const int64_t* sys_off,
                         const int32_t* active, const double* b, const double* dinv, double* x, double* r, double* p,
                         double* Ap, double rtol, int32_t maxit, int32_t cluster, int32_t* status,
@@ -364,7 +368,7 @@ typedef struct cib_rve_newton {
   double increment_relative_tolerance;
   double pcg_rtol;
   int32_t pcg_maxit;
-  int32_t cluster; /* PCG CTAs per system: 1, 2, 4 or 8 */
+  int32_t cluster; /* PCG CTAs per system (1, 2, 4, 8) and launch shape, as in cib_rve_pcg_cluster */
   const double* time_step;
   const double* macro;
   const double* w_n;

@@ -1,9 +1,10 @@
 """NumPy oracle of the explicit macro dynamics -- test infrastructure only.
 
-Restates, for a structured Hex8 bar and a linear elastic material (internal force K u):
+Restates, for a structured Hex8 bar and a linear elastic material (internal force K u) or
+a J2 Perzyna material (internal force sum B^T sigma w from the J2 oracle):
   assemble_lumped_mass_vector (row sum of the consistent mass)   src/fem/assembly/elasticity.py:73-77
   assemble_uniform_boundary_pressure (traction -p n on a face)   src/fem/assembly/load.py:40-77
-  solve_material_explicit velocity-Verlet step                   src/fem/dynamics/material.py:164-219
+  solve_material_explicit velocity-Verlet step and histories     src/fem/dynamics/material.py:89-297
 """
 
 from __future__ import annotations
@@ -11,6 +12,7 @@ from __future__ import annotations
 import numpy as np
 from scipy.sparse import coo_matrix
 
+from . import j2vp as oj
 from .j2vp import elasticity_matrix
 from .rve import b_matrices, box_mesh
 
@@ -83,3 +85,55 @@ def explicit_elastic_bar(divisions, lengths, density, young_modulus, poisson_rat
         vn[fixed] = 0.0
         u, v, a = un, vn, an
     return u, v, a
+
+
+def explicit_j2_bar(divisions, lengths, params: oj.J2Params, density: float, dt: float, steps: int, load, fixed_dofs):
+    """solve_material_explicit on a J2 Perzyna bar: ``load(t)`` is the external force
+    vector, ``fixed_dofs`` the homogeneous Dirichlet DOFs.  Returns the histories
+    (times, u, v, a, stresses, eqps, kinetic, dissipated energy, external work)."""
+    nodes, elements = box_mesh(lengths, divisions)
+    b, jw = b_matrices(nodes, elements)
+    dofs = (3 * elements[:, :, None] + np.arange(3)).reshape(-1, 24)
+    m = lumped_mass(nodes, elements, density)
+    n3, npts = 3 * nodes.shape[0], 8 * elements.shape[0]
+    fixed = np.zeros(n3, dtype=bool)
+    fixed[np.asarray(fixed_dofs)] = True
+    state = {"ep": np.zeros((npts, 6)), "q": np.zeros(npts), "vpm": np.zeros(npts)}
+    weights = jw.reshape(-1)
+
+    def assemble(u, u_prev, st):
+        eps = np.einsum("eqij,ej->eqi", b, u[dofs]).reshape(-1, 6)
+        rate = (np.einsum("eqij,ej->eqi", b, (u - u_prev)[dofs]) / dt).reshape(-1, 6)
+        out = oj.update_reference_form(params, eps, st["ep"], st["q"], st["vpm"], dt, rate)
+        if np.any(out["status"] != 0):
+            raise FloatingPointError("J2 point failure")
+        f = np.zeros(n3)
+        np.add.at(f, dofs.ravel(), np.einsum("eqij,eqi,eq->ej", b, out["stresses"].reshape(-1, 8, 6), jw).ravel())
+        new = {"ep": out["plastic_strain"], "q": out["equivalent_plastic_strain"], "vpm": out["viscoplastic_multiplier"]}
+        return f, out, new
+
+    u, v = np.zeros(n3), np.zeros(n3)
+    f_int, out, state = assemble(u, u, state)
+    external = load(0.0)
+    a = (external - f_int) / m
+    a[fixed] = 0.0
+    hist = {"times": [0.0], "u": [u], "v": [v], "a": [a], "stresses": [out["stresses"]],
+            "eqps": [out["equivalent_plastic_strain"]], "kinetic": [0.5 * np.sum(m * v * v)], "dissipated": [0.0],
+            "work": [0.0]}  # fmt: skip
+    for step in range(steps):
+        t1 = (step + 1) * dt
+        un = u + dt * v + 0.5 * dt**2 * a
+        un[fixed] = 0.0
+        f_int, out, state = assemble(un, u, state)
+        external1 = load(t1)
+        an = (external1 - f_int) / m
+        an[fixed] = 0.0
+        vn = v + 0.5 * dt * (a + an)
+        vn[fixed] = 0.0
+        hist["dissipated"].append(hist["dissipated"][-1] + dt * float(np.dot(out["dissipation"], weights)))
+        hist["work"].append(hist["work"][-1] + 0.5 * float((external + external1) @ (un - u)))
+        u, v, a, external = un, vn, an, external1
+        for key, value in (("times", t1), ("u", u), ("v", v), ("a", a), ("stresses", out["stresses"]),
+                           ("eqps", out["equivalent_plastic_strain"]), ("kinetic", 0.5 * np.sum(m * v * v))):
+            hist[key].append(value)
+    return {k: np.asarray(val) for k, val in hist.items()}

@@ -441,6 +441,89 @@ def _newmark_run(bundle, nodes, fixed, unit, amplitude, duration, dt, steps, ada
     return arrays, meta
 
 
+def _explicit_run(bundle, nodes, fixed, unit, amplitude, duration, dt, steps):
+    import math
+
+    from fem.dynamics.material import solve_material_explicit
+    from fem.materials.data import MaterialUpdateSettings
+    from fem.solvers.data import DirichletDofSet, TimeIntegrationSettings
+
+    def load(t):
+        return (amplitude * math.sin(math.pi * t / duration) if 0.0 <= t <= duration else 0.0) * unit
+
+    n_dof = 3 * nodes.shape[0]
+    sol = solve_material_explicit(
+        bundle, TimeIntegrationSettings("explicit", dt, steps, 0.0, 0.5, 0.9), np.zeros(n_dof), np.zeros(n_dof),
+        DirichletDofSet(fixed, np.zeros(fixed.size)), load, "three_dimensional",
+        MaterialUpdateSettings(50, 1.0e-10, 1.0e-12, 1.0e-10))  # fmt: skip
+    arrays = {name: np.asarray(getattr(sol, name)) for name in (
+        "times", "displacement", "velocity", "acceleration", "internal_force", "external_force", "stresses",
+        "equivalent_plastic_strain", "kinetic_energy", "free_energy", "dissipated_energy", "external_work",
+        "energy_residual", "positive_incremental_work", "negative_incremental_work", "unloading_volume_fraction",
+        "viscoplastic_active_volume_fraction", "accepted_time_steps")}  # fmt: skip
+    arrays["fixed_dofs"] = fixed
+    arrays["unit_force"] = unit
+    meta = {"amplitude": amplitude, "duration": duration, "time_step": dt, "num_steps": steps,
+            "cfl_safety_factor": 0.9, "update_settings": [50, 1.0e-10, 1.0e-12, 1.0e-10]}  # fmt: skip
+    return arrays, meta
+
+
+def make_explicit_cases():
+    """Explicit velocity-Verlet material dynamics of the reference (solve_material_explicit,
+    src/fem/dynamics/material.py:89-297) on pressure-pulse bars: J2 Perzyna at the macro
+    points (8x1x1 bar, 40 MPa half-sine), and explicit FE2 with a two-phase 4^3 RVE
+    (RVEHomogenizedMaterial) at each of the 24 points of a 3x1x1 bar; plus the reference's
+    CFL refusal (check_explicit_stability, src/fem/dynamics/stability.py:34-48)."""
+    from fem.dynamics.stability import check_explicit_stability
+    from fem.materials.linear_elastic import LinearElasticMaterial
+    from fem.materials.phased import PhasedMaterialModel, RVEPhase
+    from fem.materials.plasticity import J2ViscoplasticMaterial
+    from fem.mesh.structured import build_structured_hex8_box
+    from fem.rve import StructuredHex8RVE, build_structured_hex8_periodic_constraint
+    from fem.rve.material import RVEHomogenizedMaterial
+    from fem.solvers.data import ArmijoSettings, NonlinearNewtonSettings, TimeIntegrationSettings
+
+    sys.path.insert(0, str(REPO))
+    from concrete_impact_b200.rve_builders import draw_spheres, sphere_phase_map
+
+    cases = {}
+    mortar = J2ViscoplasticMaterial("mortar", 2200.0, 25.0e9, 0.2, 20.0e6, 2.0e9, 1.0e-3, 20.0e6, 1.0)
+    bar = {"divisions": (8, 1, 1), "lengths": (0.08, 0.01, 0.01)}
+    bundle, nodes, elements, fixed, unit, _ = _newmark_bar(bar["divisions"], bar["lengths"], mortar)
+    report = check_explicit_stability(bundle, TimeIntegrationSettings("explicit", 1.0e-6, 1, 0.0, 0.5, 0.9))
+    arrays, meta = _explicit_run(bundle, nodes, fixed, unit, 40.0e6, 20.0e-6, 1.0e-6, 60)
+    meta.update(bar=bar, material=MATERIALS["mortar"], stable_time_step=report.stable_time_step,
+                minimum_length=report.minimum_length, maximum_wave_speed=report.maximum_wave_speed)  # fmt: skip
+    try:
+        check_explicit_stability(bundle, TimeIntegrationSettings("explicit", 1.0e-5, 1, 0.0, 0.5, 0.9))
+        raise AssertionError("the reference accepted a step above its CFL bound")
+    except ValueError as error:
+        meta["cfl_violation"] = {"time_step": 1.0e-5, "message": str(error)}
+    cases["explicit_j2_bar"] = (arrays, meta)
+    aggregate = LinearElasticMaterial("aggregate", 2600.0, 50.0e9, 0.2)
+    div = (4, 4, 4)
+    rnodes, relements = build_structured_hex8_box((1.0, 1.0, 1.0), div)
+    phase = sphere_phase_map(div, draw_spheres(7))
+    frac = float(phase.mean())
+    density = 2200.0 * (1.0 - frac) + 2600.0 * frac
+    phased = PhasedMaterialModel("mortar__aggregate", (RVEPhase("matrix", mortar), RVEPhase("inclusion", aggregate)),
+                                 np.repeat(phase, 8), density)  # fmt: skip
+    rve_newton = NonlinearNewtonSettings(25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, ArmijoSettings(enabled=False))
+    model = StructuredHex8RVE(rnodes, relements, div, phased, build_structured_hex8_periodic_constraint(rnodes, div),
+                              rve_newton, element_phase_ids=phase, phase_names=("matrix", "inclusion"))  # fmt: skip
+    fe2_bar = {"divisions": (3, 1, 1), "lengths": (0.03, 0.01, 0.01)}
+    material = RVEHomogenizedMaterial(model, "two_phase_rve")
+    bundle, nodes, elements, fixed, unit, _ = _newmark_bar(fe2_bar["divisions"], fe2_bar["lengths"], material)
+    report = check_explicit_stability(bundle, TimeIntegrationSettings("explicit", 1.0e-6, 1, 0.0, 0.5, 0.9))
+    arrays, meta = _explicit_run(bundle, nodes, fixed, unit, 40.0e6, 10.0e-6, 1.0e-6, 12)
+    arrays["element_phase"] = phase
+    meta.update(bar=fe2_bar, stable_time_step=report.stable_time_step,
+                rve={"divisions": div, "seed": 7, "density": density,
+                     "newton": [25, 1.0e-6, 1.0e-8, 1.0e-14, 1.0e-10, False]})  # fmt: skip
+    cases["explicit_fe2_bar"] = (arrays, meta)
+    return cases
+
+
 def make_newmark_cases():
     """Implicit Newmark material dynamics of the reference (solve_material_implicit_newmark)
     on small pressure-pulse bars: J2 Perzyna at the macro points (fixed steps; adaptive
@@ -611,7 +694,7 @@ def make_rno_energy_cases(src: str):
     return {"rno_energy_c48": (arrays, meta)}
 
 
-GROUPS = ("j2", "rve", "newmark", "ogrid", "rno_energy", "rve_batch", "rve_path")
+GROUPS = ("j2", "rve", "newmark", "ogrid", "rno_energy", "rve_batch", "rve_path", "explicit")
 
 
 def main() -> None:
@@ -644,6 +727,8 @@ def main() -> None:
         cases.update(make_rve_batch_cases())
     if "rve_path" in groups:
         cases.update(make_rve_path_cases())
+    if "explicit" in groups:
+        cases.update(make_explicit_cases())
     path = HERE / "manifest.json"
     manifest = json.loads(path.read_text()) if path.exists() and args.only else {}
     for name, (arrays, meta) in cases.items():

@@ -47,3 +47,30 @@ def test_elastic_wave_front_speed() -> None:
     mid = ux[np.isclose(nodes[:, 0], 0.3)]  # reached
     assert np.abs(front).max() < 1e-3 * np.abs(mid).max()
     assert np.all(mid < 0)
+
+
+def test_explicit_j2_oracle_reproduces_reference_run() -> None:
+    """The oracle's velocity Verlet with J2 points reproduces the reference's own
+    solve_material_explicit run (tests/golden explicit_j2_bar) to 1e-11 of each history's
+    maximum; its lumped mass and face load are the reference's."""
+    import math
+
+    from oracle import j2vp as oj
+    from tests.conftest import load_case
+
+    g, meta = load_case("explicit_j2_bar")
+    div, lengths = tuple(meta["bar"]["divisions"]), tuple(meta["bar"]["lengths"])
+    nodes, elements = box_mesh(lengths, div)
+    np.testing.assert_allclose(of.face_pressure_force(nodes, lengths, div), g["unit_force"], rtol=0, atol=1e-18)
+    amp, dur = meta["amplitude"], meta["duration"]
+
+    def load(t):
+        return (amp * math.sin(math.pi * t / dur) if 0.0 <= t <= dur else 0.0) * g["unit_force"]
+
+    h = of.explicit_j2_bar(div, lengths, oj.mortar_params(), meta["material"]["density"], meta["time_step"],
+                           meta["num_steps"], load, g["fixed_dofs"])  # fmt: skip
+    for ours, ref in (("u", "displacement"), ("v", "velocity"), ("a", "acceleration"), ("stresses", "stresses"),
+                      ("eqps", "equivalent_plastic_strain"), ("kinetic", "kinetic_energy"),
+                      ("dissipated", "dissipated_energy"), ("work", "external_work")):
+        np.testing.assert_allclose(h[ours], g[ref], rtol=0, atol=1e-11 * np.abs(g[ref]).max(), err_msg=ref)
+    assert g["equivalent_plastic_strain"].max() > 1e-4

@@ -69,9 +69,39 @@ def test_auto_and_tuned_cluster_choice() -> None:
     assert small.cluster == 1
     batch.macro.copy_(torch.full((2, 6), 1.0e-3, dtype=torch.float64, device=batch.device))
     batch.dt.fill_(5.0e-6)
-    out = R.tune_pcg_cluster(batch, UPDATE)
-    assert set(out["ms"]) == {1, 2, 4, 8} and out["cluster"] in out["ms"]
-    assert batch.cluster == out["cluster"]
+    out = R.tune_pcg_cluster(batch, UPDATE, persist=False)
+    expected = {"1/0"} | {f"{c}/{s}" for c in (2, 4, 8) for s in range(4)}
+    assert set(out["ms"]) == expected and f"{out['cluster']}/{out['shape']}" in out["ms"]
+    assert (batch.cluster, batch.pcg_shape) == (out["cluster"], out["shape"])
+
+
+def test_pcg_launch_shapes_agree(tmp_path, monkeypatch) -> None:
+    """Every launch shape of the cluster PCG solves the same systems (same iteration
+    counts up to the rounding of the CTA sums, solutions within 1e-9); the tuner's choice
+    is persisted per edge mix and reused without timing."""
+    models = _models([8, 16], 64)
+    batch = R.RVEBatch(models, precision=64, linear_solver=R.LinearSolverOptions(cluster=4))
+    batch.macro.copy_(torch.full((2, 6), 1.0e-3, dtype=torch.float64, device=batch.device))
+    batch.dt.fill_(5.0e-6)
+    b = batch.batch_struct(UPDATE)
+    batch.residual(b, batch.w, None, None)
+    sols = []
+    for shape in range(4):
+        batch.pcg_shape = shape
+        batch.x.zero_()
+        batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, batch.nrve, batch.sys_rve, batch.sys_off,
+                  batch.pcg_status, batch.pcg_iters, batch.pcg_rel, batch.pcg_xnorm)  # fmt: skip
+        torch.cuda.synchronize()
+        assert torch.all(batch.pcg_status == 0)
+        sols.append((batch.x.cpu().numpy(), batch.pcg_iters.cpu().numpy()))
+    for x, its in sols[1:]:
+        np.testing.assert_allclose(x, sols[0][0], rtol=1e-9, atol=1e-9 * np.abs(sols[0][0]).max())
+        assert np.abs(its - sols[0][1]).max() <= 2
+    monkeypatch.setenv("CIB_TUNING_CACHE", str(tmp_path / "tuning.json"))
+    first = R.tune_pcg_cluster(batch, UPDATE)
+    assert not first["cached"] and (tmp_path / "tuning.json").exists()
+    again = R.tune_pcg_cluster(R.RVEBatch(models, precision=64), UPDATE)
+    assert again["cached"] and (again["cluster"], again["shape"]) == (first["cluster"], first["shape"])
 
 
 def test_saved_state_resumes_bitwise(tmp_path) -> None:
