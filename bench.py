@@ -332,8 +332,9 @@ def run_ours(args: argparse.Namespace) -> None:
         torch.cuda.empty_cache()
         return total_ms, kernel_ms, failures, active
 
-    def e2e_timed(dtype):
-        """Host-resident batch: pinned host SoA in, pinned host SoA + tangent out."""
+    def e2e_timed(dtype, compact: bool = False):
+        """Host-resident batch: pinned host SoA in, pinned host SoA + tangent out (36 rows,
+        or the 8-row compact form)."""
         de_d, st_d = make_inputs(dtype)
         de_h = de_d.cpu().pin_memory()
         st_h = batched.SoAState(st_d.stress.cpu().pin_memory(), st_d.plastic_strain.cpu().pin_memory(),
@@ -342,8 +343,8 @@ def run_ours(args: argparse.Namespace) -> None:
         torch.cuda.empty_cache()
         out_h = batched.SoAState(torch.empty((6, n), dtype=dtype).pin_memory(), torch.empty((6, n), dtype=dtype).pin_memory(),
                                  torch.empty(n, dtype=torch.float64).pin_memory())  # fmt: skip
-        tan_h = torch.empty((36, n), dtype=dtype).pin_memory()
-        pipe = batched.J2HostPipeline(material, settings, dtype, chunk=1 << 20)
+        tan_h = torch.empty((8 if compact else 36, n), dtype=dtype).pin_memory()
+        pipe = batched.J2HostPipeline(material, settings, dtype, chunk=1 << 20, compact_tangent=compact)
         pipe.run(dt, de_h, st_h, out_h, tan_h)  # warm-up
         torch.cuda.synchronize()
         if dist is not None:
@@ -353,7 +354,7 @@ def run_ours(args: argparse.Namespace) -> None:
         for _ in range(args.e2e_steps):
             fails = max(fails, pipe.run(dt, de_h, st_h, out_h, tan_h))
         elapsed = time.perf_counter() - t0
-        h2d, d2h = batched.J2HostPipeline.bytes_per_point(dtype, True)
+        h2d, d2h = batched.J2HostPipeline.bytes_per_point(dtype, True, compact)
         launches = math.ceil(n / pipe.chunk) * args.e2e_steps
         del pipe, de_h, st_h, out_h, tan_h
         torch.cuda.empty_cache()
@@ -364,6 +365,12 @@ def run_ours(args: argparse.Namespace) -> None:
         total64, kms64, fail64, _ = device_timed(torch.float64)
         total32, kms32, fail32, _ = device_timed(torch.float32)
     e2e_s, h2d_b, d2h_b, e2e_fail, e2e_launches = e2e_timed(torch.float64)
+    e2e_more = {}
+    for key, dtype, compact in (("f64_compact_tangent", torch.float64, True), ("f32", torch.float32, False),
+                                ("f32_compact_tangent", torch.float32, True)):  # fmt: skip
+        secs, hb, db, fl, _ = e2e_timed(dtype, compact)
+        e2e_fail = max(e2e_fail, fl)
+        e2e_more[key] = (secs, hb, db)
 
     def reduce_max(x: float) -> float:
         return max_over_ranks(x, dist, dev)
@@ -371,6 +378,7 @@ def run_ours(args: argparse.Namespace) -> None:
     total64 = reduce_max(total64)
     total32 = reduce_max(total32)
     e2e_s = reduce_max(e2e_s)
+    e2e_more = {k: (reduce_max(v[0]), v[1], v[2]) for k, v in e2e_more.items()}
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -404,7 +412,7 @@ def run_ours(args: argparse.Namespace) -> None:
                      "peak_kind": f"{peak_kind} (copy bandwidth, burst)",
                      "traffic": None if t64 is None else t64 * n,
                      "algorithmic_bytes_per_launch": BYTES_PER_POINT["f64"] * n,
-                     "kernel": "j2vp_soa_kernel<double,2,true>", "mean_launch_ms": k64},  # fmt: skip
+                     "kernel": "j2vp_soa_kernel<double,2,1>", "mean_launch_ms": k64},  # fmt: skip
         "variants": {"f32": {"value": value32, "unit": UNIT, "ms_per_step": total32 / args.steps,
                              "roofline": {"achieved": ach32, "peak": peak, "frac": ach32 / peak,
                                           "traffic": None if ncu_traffic("f32") is None else ncu_traffic("f32") * n,
@@ -413,7 +421,13 @@ def run_ours(args: argparse.Namespace) -> None:
                              "dtype": "f32 state and tangent, f64 equivalent plastic strain"}},  # fmt: skip
         "e2e": {"value": world * n * args.e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d_b,
                 "d2h_bytes_per_step": d2h_b, "path": "J2HostPipeline: pinned host SoA -> cib_j2vp_update_soa_f64 -> pinned host",
-                "steps": args.e2e_steps, "gpu_launches": e2e_launches},  # fmt: skip
+                "steps": args.e2e_steps, "gpu_launches": e2e_launches,
+                "variants": {k: {"value": world * n * args.e2e_steps / v[0], "h2d_bytes_per_step": v[1],
+                                 "d2h_bytes_per_step": v[2],
+                                 "path": ("J2HostPipeline, compact tangent (n, f, c: 8 values instead of 36)"
+                                          if "compact" in k else "J2HostPipeline") + (", FP32 state" if "f32" in k
+                                                                                      else "")}
+                             for k, v in e2e_more.items()}},  # fmt: skip
         "clocks": clocks.summary(),
         "cpu_baseline": cpu_line,
     }

@@ -201,6 +201,8 @@ _I = ctypes.c_int
 SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_j2vp_update_soa_f64": (_I, [_P, _P, _I64, _I64, _D] + [_P] * 10),
     "cib_j2vp_update_soa_f32": (_I, [_P, _P, _I64, _I64, _D] + [_P] * 10),
+    "cib_j2vp_update_soa_compact_f64": (_I, [_P, _P, _I64, _I64, _D] + [_P] * 10),
+    "cib_j2vp_update_soa_compact_f32": (_I, [_P, _P, _I64, _I64, _D] + [_P] * 10),
     "cib_j2vp_update": (_I, [_P, _P, _I64, _D] + [_P] * 16),
     "cib_j2vp_diagnose_point": (_I, [_P, _P, _I64, _D, _P, _P, _P, _P, _I64, _P, _P]),
     "cib_linear_elastic_update": (_I, [_D, _D, _I64, _D] + [_P] * 8),

@@ -49,13 +49,29 @@ class SoAState:
         )
 
 
-def _entry(dtype: torch.dtype):
+def _entry(dtype: torch.dtype, compact: bool = False):
     lib = _native.load_library()
     if dtype == torch.float64:
-        return lib.cib_j2vp_update_soa_f64
+        return lib.cib_j2vp_update_soa_compact_f64 if compact else lib.cib_j2vp_update_soa_f64
     if dtype == torch.float32:
-        return lib.cib_j2vp_update_soa_f32
+        return lib.cib_j2vp_update_soa_compact_f32 if compact else lib.cib_j2vp_update_soa_f32
     raise TypeError(f"unsupported dtype {dtype}; use float32 or float64")
+
+
+def expand_compact_tangent(compact: torch.Tensor, material: J2ViscoplasticMaterial) -> torch.Tensor:
+    """(36, n) consistent tangent from the compact (8, n) rows n (6), f, c:
+    C = K 1(x)1 + f P + c n(x)n (plasticity.py:929-963 in factored form)."""
+    e, nu = float(material.young_modulus), float(material.poisson_ratio)
+    bulk = e / (3.0 * (1.0 - 2.0 * nu))
+    n, f, c = compact[:6], compact[6], compact[7]
+    p = torch.zeros((6, 6), dtype=compact.dtype, device=compact.device)
+    p[:3, :3] = -1.0 / 3.0
+    p[range(3), range(3)] = 2.0 / 3.0
+    p[range(3, 6), range(3, 6)] = 0.5
+    vol = torch.zeros((6, 6), dtype=compact.dtype, device=compact.device)
+    vol[:3, :3] = bulk
+    out = vol.reshape(36, 1) + p.reshape(36, 1) * f[None, :] + c[None, :] * (n[:, None, :] * n[None, :, :]).reshape(36, -1)
+    return out
 
 
 def launch_j2vp_soa(
@@ -73,7 +89,8 @@ def launch_j2vp_soa(
     """Asynchronous launch (no host sync).  ``flags[0]`` receives the lowest failing index.
 
     The (6, ld) / (36, ld) tensors may hold more columns than the ``count`` points updated
-    (default: all ld columns); the leading dimension is the tensors' row length.
+    (default: all ld columns); the leading dimension is the tensors' row length.  A tangent
+    of 8 rows receives the compact form (n (6), f, c; ``expand_compact_tangent``).
     """
     ld = int(dstrain.shape[1])
     n = ld if count is None else int(count)
@@ -85,11 +102,13 @@ def launch_j2vp_soa(
     for t in (state_n.eqps, state.eqps):
         if t.shape[0] < n or t.dtype != torch.float64 or not t.is_contiguous():
             raise ValueError("equivalent plastic strain must be a contiguous float64 tensor of >= count points.")
-    if tangent is not None and (tangent.shape != (36, ld) or not tangent.is_contiguous() or tangent.dtype != dstrain.dtype):
-        raise ValueError("tangent must be a contiguous (36, ld) tensor of the state dtype.")
+    if tangent is not None and (tangent.shape not in ((36, ld), (8, ld)) or not tangent.is_contiguous()
+                                or tangent.dtype != dstrain.dtype):  # fmt: skip
+        raise ValueError("tangent must be a contiguous (36, ld) (full) or (8, ld) (compact) tensor of the state dtype.")
+    compact = tangent is not None and tangent.shape[0] == 8
     mat_c = _native.material_struct(material)
     set_c = _native.settings_struct(settings)
-    code = _entry(dstrain.dtype)(
+    code = _entry(dstrain.dtype, compact)(
         ctypes.byref(mat_c), ctypes.byref(set_c), n, ld, float(time_step),
         dstrain.data_ptr(), state_n.stress.data_ptr(), state_n.plastic_strain.data_ptr(), state_n.eqps.data_ptr(),
         state.stress.data_ptr(), state.plastic_strain.data_ptr(), state.eqps.data_ptr(), _native.ptr(tangent),
@@ -168,16 +187,20 @@ class J2HostPipeline:
     Chunks of ``chunk`` points are copied in on one stream, updated on a second and
     copied out on a third, with two device buffer sets in flight.  Results land in the
     caller's pinned host output arrays; ``run`` returns after the last copy finished.
+    ``compact_tangent`` returns the tangent as 8 rows (n, f, c) instead of 36, which cuts
+    the device-to-host traffic per point from 48 to 20 values.
     """
 
     def __init__(self, material: J2ViscoplasticMaterial, settings: MaterialUpdateSettings, dtype: torch.dtype,
-                 chunk: int = 1 << 20, with_tangent: bool = True, buffers: int = 2) -> None:  # fmt: skip
+                 chunk: int = 1 << 20, with_tangent: bool = True, buffers: int = 2,
+                 compact_tangent: bool = False) -> None:  # fmt: skip
         self.device = _native.require_cuda()
         self.material = material
         self.settings = settings
         self.dtype = dtype
         self.chunk = int(chunk)
         self.with_tangent = with_tangent
+        self.tangent_rows = 8 if compact_tangent else 36
         self.h2d = torch.cuda.Stream()
         self.compute = torch.cuda.Stream()
         self.d2h = torch.cuda.Stream()
@@ -188,7 +211,8 @@ class J2HostPipeline:
                     "de": torch.empty((6, self.chunk), dtype=dtype, device=self.device),
                     "in": SoAState.empty(self.chunk, dtype, self.device),
                     "out": SoAState.empty(self.chunk, dtype, self.device),
-                    "tan": torch.empty((36, self.chunk), dtype=dtype, device=self.device) if with_tangent else None,
+                    "tan": (torch.empty((self.tangent_rows, self.chunk), dtype=dtype, device=self.device)
+                            if with_tangent else None),
                     "loaded": torch.cuda.Event(),
                     "computed": torch.cuda.Event(),
                     "drained": torch.cuda.Event(),
@@ -198,10 +222,11 @@ class J2HostPipeline:
         self.flags = _flags(self.device)
 
     @staticmethod
-    def bytes_per_point(dtype: torch.dtype, with_tangent: bool) -> tuple[int, int]:
+    def bytes_per_point(dtype: torch.dtype, with_tangent: bool, compact_tangent: bool = False) -> tuple[int, int]:
         """(host-to-device, device-to-host) bytes per point."""
         w = 8 if dtype == torch.float64 else 4
-        return 18 * w + 8, (12 + (36 if with_tangent else 0)) * w + 8
+        rows = (8 if compact_tangent else 36) if with_tangent else 0
+        return 18 * w + 8, (12 + rows) * w + 8
 
     def run(self, time_step: float, dstrain: torch.Tensor, state_n: SoAState, state: SoAState,
             tangent: torch.Tensor | None) -> int:  # fmt: skip
@@ -243,7 +268,7 @@ class J2HostPipeline:
             rows_out(state.plastic_strain, buf["out"].plastic_strain, 6, w)
             rows_out(state.eqps, buf["out"].eqps, 1, 8)
             if tangent is not None and buf["tan"] is not None:
-                rows_out(tangent, buf["tan"], 36, w)
+                rows_out(tangent, buf["tan"], self.tangent_rows, w)
             buf["drained"].record(self.d2h)
         self.d2h.synchronize()
         return int(self.flags[0].item())

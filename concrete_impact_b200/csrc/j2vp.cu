@@ -84,7 +84,10 @@ __device__ __forceinline__ void stq(double* __restrict__ p, const double (&in)[V
 // ---------------------------------------------------------------------------------------
 // Streaming SoA kernel.  Component c of point p lives at [c * stride + p].  Points
 // [0, count) of the (already offset) pointers are processed, VEC per thread.
-template <typename T, int VEC, bool TAN>
+// TAN: 0 no tangent, 1 the full 6x6 consistent tangent (36 rows), 2 the compact tangent
+// (8 rows: flow direction n (6), f, c with C = K 1(x)1 + f P + c n(x)n, P the deviatoric
+// projector in engineering-shear Voigt form; an elastic point has n = 0, f = 2G, c = 0).
+template <typename T, int VEC, int TAN>
 __global__ void __launch_bounds__(256) j2vp_soa_kernel(
     const J2Consts<T> c, const T dt, const int64_t nvec, const int64_t stride, const T* __restrict__ de,
     const T* __restrict__ s0, const T* __restrict__ ep0, const double* __restrict__ q0, T* __restrict__ s1,
@@ -153,7 +156,24 @@ __global__ void __launch_bounds__(256) j2vp_soa_kernel(
       stv<T, VEC>(ep1 + k * stride + p0, ep[k]);
     }
     stq<VEC>(q1 + p0, q);
-    if (TAN) {
+    if (TAN == 2) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        T row[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) row[j] = act[j] ? nn[i][j] : (T)0;
+        stv<T, VEC>(tan + (int64_t)i * stride + p0, row);
+      }
+      T rf[VEC], rc[VEC];
+#pragma unroll
+      for (int j = 0; j < VEC; ++j) {
+        rf[j] = act[j] ? tf[j] : (T)2 * c.G;
+        rc[j] = act[j] ? tc[j] : (T)0;
+      }
+      stv<T, VEC>(tan + (int64_t)6 * stride + p0, rf);
+      stv<T, VEC>(tan + (int64_t)7 * stride + p0, rc);
+    }
+    if (TAN == 1) {
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
 #pragma unroll
@@ -422,7 +442,7 @@ __global__ void __launch_bounds__(128) linear_elastic_kernel(const ElasticArgs a
 // ---------------------------------------------------------------------------------------
 // Host launchers.
 
-template <typename T, int VEC, bool TAN>
+template <typename T, int VEC, int TAN>
 static int launch_soa(const J2Consts<T>& c, T dt, int64_t count, int64_t stride, const T* de, const T* s0,
                       const T* ep0, const double* q0, T* s1, T* ep1, double* q1, T* tan,
                       unsigned long long* ff, cudaStream_t st, int64_t index_offset = 0) {
@@ -438,18 +458,24 @@ static int launch_soa(const J2Consts<T>& c, T dt, int64_t count, int64_t stride,
 template <typename T, int VEC>
 static int run_soa(const cib_j2vp_material* m, const cib_update_settings* s, int64_t n, int64_t ld, double dt,
                    const T* de, const T* s0, const T* ep0, const double* q0, T* s1, T* ep1, double* q1, T* tan,
-                   unsigned long long* ff, void* stream) {
+                   unsigned long long* ff, void* stream, bool compact = false) {
   if (!m || !s || n < 0 || ld < n || !de || !s0 || !ep0 || !q0 || !s1 || !ep1 || !q1) return CIB_EINVAL;
+  if (compact && !tan) return CIB_EINVAL;
   if (n == 0) return CIB_OK;
   const J2Consts<T> c = make_j2_consts<T>(*m, *s);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int mode = tan ? (compact ? 2 : 1) : 0;
   const bool aligned = (ld % VEC == 0) && aligned16(de) && aligned16(s0) && aligned16(ep0) && aligned16(q0) &&
                        aligned16(s1) && aligned16(ep1) && aligned16(q1) && (tan == nullptr || aligned16(tan));
   int64_t done = 0;
   if (aligned) {
     const int64_t main = n - n % VEC;
-    const int rc = tan ? launch_soa<T, VEC, true>(c, (T)dt, main, ld, de, s0, ep0, q0, s1, ep1, q1, tan, ff, st)
-                       : launch_soa<T, VEC, false>(c, (T)dt, main, ld, de, s0, ep0, q0, s1, ep1, q1, tan, ff, st);
+    int rc;
+    switch (mode) {
+      case 2: rc = launch_soa<T, VEC, 2>(c, (T)dt, main, ld, de, s0, ep0, q0, s1, ep1, q1, tan, ff, st); break;
+      case 1: rc = launch_soa<T, VEC, 1>(c, (T)dt, main, ld, de, s0, ep0, q0, s1, ep1, q1, tan, ff, st); break;
+      default: rc = launch_soa<T, VEC, 0>(c, (T)dt, main, ld, de, s0, ep0, q0, s1, ep1, q1, tan, ff, st); break;
+    }
     if (rc != CIB_OK) return rc;
     done = main;
   }
@@ -457,10 +483,18 @@ static int run_soa(const cib_j2vp_material* m, const cib_update_settings* s, int
   // Scalar path for the remaining points (pointers shifted by o; failure indices are
   // reported unshifted through index_offset).
   const int64_t o = done;
-  return tan ? launch_soa<T, 1, true>(c, (T)dt, n - o, ld, de + o, s0 + o, ep0 + o, q0 + o, s1 + o, ep1 + o, q1 + o,
-                                      tan + o, ff, st, o)
-             : launch_soa<T, 1, false>(c, (T)dt, n - o, ld, de + o, s0 + o, ep0 + o, q0 + o, s1 + o, ep1 + o, q1 + o,
-                                       nullptr, ff, st, o);
+  T* to = tan ? tan + o : nullptr;
+  switch (mode) {
+    case 2:
+      return launch_soa<T, 1, 2>(c, (T)dt, n - o, ld, de + o, s0 + o, ep0 + o, q0 + o, s1 + o, ep1 + o, q1 + o, to, ff,
+                                 st, o);
+    case 1:
+      return launch_soa<T, 1, 1>(c, (T)dt, n - o, ld, de + o, s0 + o, ep0 + o, q0 + o, s1 + o, ep1 + o, q1 + o, to, ff,
+                                 st, o);
+    default:
+      return launch_soa<T, 1, 0>(c, (T)dt, n - o, ld, de + o, s0 + o, ep0 + o, q0 + o, s1 + o, ep1 + o, q1 + o, to, ff,
+                                 st, o);
+  }
 }
 
 }  // namespace cib
@@ -483,6 +517,26 @@ extern "C" int cib_j2vp_update_soa_f32(const cib_j2vp_material* material, const 
                                        unsigned long long* first_failure, void* stream) {
   return run_soa<float, 4>(material, settings, n, ld, time_step, dstrain, stress_n, plastic_strain_n, eqps_n, stress,
                            plastic_strain, eqps, tangent, first_failure, stream);
+}
+
+extern "C" int cib_j2vp_update_soa_compact_f64(const cib_j2vp_material* material, const cib_update_settings* settings,
+                                               int64_t n, int64_t ld, double time_step, const double* dstrain,
+                                               const double* stress_n, const double* plastic_strain_n,
+                                               const double* eqps_n, double* stress, double* plastic_strain,
+                                               double* eqps, double* tangent8, unsigned long long* first_failure,
+                                               void* stream) {
+  return run_soa<double, 2>(material, settings, n, ld, time_step, dstrain, stress_n, plastic_strain_n, eqps_n, stress,
+                            plastic_strain, eqps, tangent8, first_failure, stream, true);
+}
+
+extern "C" int cib_j2vp_update_soa_compact_f32(const cib_j2vp_material* material, const cib_update_settings* settings,
+                                               int64_t n, int64_t ld, double time_step, const float* dstrain,
+                                               const float* stress_n, const float* plastic_strain_n,
+                                               const double* eqps_n, float* stress, float* plastic_strain,
+                                               double* eqps, float* tangent8, unsigned long long* first_failure,
+                                               void* stream) {
+  return run_soa<float, 4>(material, settings, n, ld, time_step, dstrain, stress_n, plastic_strain_n, eqps_n, stress,
+                           plastic_strain, eqps, tangent8, first_failure, stream, true);
 }
 
 extern "C" int cib_j2vp_update(const cib_j2vp_material* material, const cib_update_settings* settings, int64_t n,

@@ -676,9 +676,9 @@ def _solve_batch_step_graph(batch: RVEBatch, newton: NonlinearNewtonSettings, up
             raise failure_context(r, info)
         raise MaterialPointConvergenceError("RVE material point failed.", "material_point_failure",
                                             {"rve_index": r, "point_id": info})  # fmt: skip
-    if error == 3:
-        raise RVEEquilibriumError("maximum_iterations_exceeded", _failure_diag(batch, r, int(iw[0]), rnorm[r], tol[r],
-                                                                               inc[r], inc_tol[r]))  # fmt: skip
+    if error == 3:  # found by the check of the last iteration; the loop counter was advanced after it
+        raise RVEEquilibriumError("maximum_iterations_exceeded", _failure_diag(batch, r, int(iw[0]) - 1, rnorm[r],
+                                                                               tol[r], inc[r], inc_tol[r]))  # fmt: skip
     if error == 2:
         d = _failure_diag(batch, r, int(iw[0]) - 1, rnorm[r], tol[r], float(inc[r]), inc_tol[r])
         d["linear_solver_status"] = info

@@ -147,6 +147,25 @@ int cib_j2vp_update_soa_f32(const cib_j2vp_material* material, const cib_update_
                             float* plastic_strain, double* eqps, float* tangent,
                             unsigned long long* first_failure, void* stream);
 
+/* The same update with the consistent tangent in compact form: tangent8 has 8 rows
+ * [r * ld + p]: the flow direction n (6), f and c, such that
+ *   C = K 1 (x) 1 + f P + c n (x) n
+ * with K the bulk modulus and P the deviatoric projector in engineering-shear Voigt form
+ * (P_ij = delta_ij - 1/3 for i, j < 3, P_ii = 1/2 for i >= 3, else 0) -- the factored form
+ * of the reference's _j2_viscoplastic_consistent_tangent (plasticity.py:929-963).  An
+ * elastic point has n = 0, f = 2G, c = 0.  8 instead of 36 tangent values per point. */
+int cib_j2vp_update_soa_compact_f64(const cib_j2vp_material* material, const cib_update_settings* settings,
+                                    int64_t n, int64_t ld, double time_step, const double* dstrain,
+                                    const double* stress_n, const double* plastic_strain_n, const double* eqps_n,
+                                    double* stress, double* plastic_strain, double* eqps, double* tangent8,
+                                    unsigned long long* first_failure, void* stream);
+
+int cib_j2vp_update_soa_compact_f32(const cib_j2vp_material* material, const cib_update_settings* settings,
+                                    int64_t n, int64_t ld, double time_step, const float* dstrain,
+                                    const float* stress_n, const float* plastic_strain_n, const double* eqps_n,
+                                    float* stress, float* plastic_strain, double* eqps, float* tangent8,
+                                    unsigned long long* first_failure, void* stream);
+
 /* --- Return map, reference form (array of structures, float64) -------------------------
  * strain (n,6), optional strain_rate (n,6) (NULL = None), state plastic_strain (n,6),
  * equivalent_plastic_strain (n), viscoplastic_multiplier (n).  Outputs: stress (n,6),

@@ -323,3 +323,43 @@ def test_host_pipeline_equals_device_path(dtype: torch.dtype) -> None:
     assert torch.equal(out.plastic_strain, dev_new.plastic_strain.cpu())
     assert torch.equal(out.eqps, dev_new.eqps.cpu())
     assert torch.equal(tan, dev_tan.cpu())
+
+
+@pytest.mark.parametrize("dtype,rtol", [(torch.float64, 1e-12), (torch.float32, 2e-6)])
+@pytest.mark.parametrize("n", [5, 100_003])
+def test_compact_tangent_expands_to_the_full_tangent(dtype: torch.dtype, rtol: float, n: int) -> None:
+    """cib_j2vp_update_soa_compact_*: the same state as the full-tangent entry, and its 8
+    rows (n, f, c) give the full consistent tangent C = K 1(x)1 + f P + c n(x)n."""
+    inp, de, st = _soa_inputs(n, 21, dtype)
+    new, tan = batched.j2vp_update_soa(_mortar(), SETTINGS, inp["dt"], de, st)
+    flags = torch.full((1,), -1, dtype=torch.int64, device=de.device)
+    out = batched.SoAState.empty(n, dtype, de.device)
+    compact = torch.empty((8, n), dtype=dtype, device=de.device)
+    batched.launch_j2vp_soa(_mortar(), SETTINGS, inp["dt"], de, st, out, compact, flags)
+    torch.cuda.synchronize()
+    assert int(flags[0]) == -1
+    assert torch.equal(out.stress, new.stress) and torch.equal(out.eqps, new.eqps)
+    full = batched.expand_compact_tangent(compact.double(), _mortar()).cpu().numpy()
+    ref = tan.double().cpu().numpy()
+    assert np.abs(full - ref).max() <= rtol * np.abs(ref).max()
+    plastic = compact[7].cpu().numpy() != 0.0
+    assert 0.1 < plastic.mean() < 0.9  # both branches occur
+
+
+def test_host_pipeline_compact_tangent() -> None:
+    n = 70_001
+    inp, de, st = _soa_inputs(n, 9, torch.float64)
+    flags = torch.full((1,), -1, dtype=torch.int64, device=de.device)
+    dev_out = batched.SoAState.empty(n, torch.float64, de.device)
+    dev_c = torch.empty((8, n), dtype=torch.float64, device=de.device)
+    batched.launch_j2vp_soa(_mortar(), SETTINGS, inp["dt"], de, st, dev_out, dev_c, flags)
+    pipe = batched.J2HostPipeline(_mortar(), SETTINGS, torch.float64, chunk=1 << 15, compact_tangent=True)
+    de_h = de.cpu().pin_memory()
+    st_h = batched.SoAState(st.stress.cpu().pin_memory(), st.plastic_strain.cpu().pin_memory(), st.eqps.cpu().pin_memory())
+    out = batched.SoAState(torch.empty((6, n), dtype=torch.float64).pin_memory(),
+                           torch.empty((6, n), dtype=torch.float64).pin_memory(),
+                           torch.empty(n, dtype=torch.float64).pin_memory())  # fmt: skip
+    tan = torch.empty((8, n), dtype=torch.float64).pin_memory()
+    assert pipe.run(inp["dt"], de_h, st_h, out, tan) == -1
+    assert torch.equal(out.stress, dev_out.stress.cpu()) and torch.equal(tan, dev_c.cpu())
+    assert batched.J2HostPipeline.bytes_per_point(torch.float64, True, True) == (152, 168)
