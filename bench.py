@@ -125,14 +125,16 @@ def run_reference(args: argparse.Namespace) -> None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded; no dataset involved)",
-        "config": {"workload": WORKLOAD, "points": args.points, "parallelism": "host process pool"},
+        "config": {"workload": WORKLOAD, "points_per_gpu": args.points, "parallelism": f"host process pool x{cores}",
+                   "sample_points_per_step": done},
         "cpu_baseline": {
             "value": value,
             "unit": UNIT,
             "cores": cores,
             "kind": "port",
-            "sample": f"{per_task} points per worker per step x {cores} spawn workers; per-point loop port of "
-            "J2ViscoplasticMaterial.update (strain_rates=None, tangent) -- oracle/j2vp_loop.py",
+            "sample": f"{per_task} points per worker per step x {cores} spawn workers = {done} points per step, a "
+            "bounded sample of the 16,777,216-point workload; per-point loop port of J2ViscoplasticMaterial.update "
+            "(strain_rates=None, tangent) -- oracle/j2vp_loop.py",
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -177,10 +177,18 @@ __device__ __forceinline__ void allgather8(const T mine[3], T u[8][3]) {
     for (int d = 0; d < 3; ++d) u[b][d] = __shfl_sync(FULL_MASK, mine[d], base + b);
 }
 
+// Index arithmetic avoids integer division by the runtime box sizes where it can (a
+// division or remainder by a runtime divisor costs tens of instructions, and these run per
+// Gauss point in every residual pass and every CG iteration): wraps are conditional
+// subtractions, and local element indices are 32-bit (an RVE has far fewer than 2^31).
+__device__ __forceinline__ int wrap_up(int i, int n) { return i >= n ? i - n : i; }      // i in [0, 2n)
+__device__ __forceinline__ int wrap_down(int i, int n) { return i < 0 ? i + n : i; }     // i in [-n, n)
+
+// Periodic batch node of physical node (i, j, k), 0 <= i <= nx etc.
 __device__ __forceinline__ int64_t periodic_node(const RveDesc& d, int i, int j, int k) {
-  i %= d.nx;
-  j %= d.ny;
-  k %= d.nz;
+  i = wrap_up(i, d.nx);
+  j = wrap_up(j, d.ny);
+  k = wrap_up(k, d.nz);
   return d.eoff + i + (int64_t)d.nx * (j + (int64_t)d.ny * k);
 }
 
@@ -190,9 +198,11 @@ __device__ __forceinline__ int64_t element_node(const RveDesc& d, int i, int j, 
 }
 
 __device__ __forceinline__ void local_ijk(const RveDesc& d, int64_t le, int& i, int& j, int& k) {
-  i = (int)(le % d.nx);
-  j = (int)((le / d.nx) % d.ny);
-  k = (int)(le / ((int64_t)d.nx * d.ny));
+  const int l = (int)le;
+  const int row = l / d.nx;  // j + ny k
+  i = l - row * d.nx;
+  k = row / d.ny;
+  j = row - k * d.ny;
 }
 
 // CTA-wide sum of NV doubles (fixed order: warp tree, then warp 0 over warps).
@@ -355,34 +365,29 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_residual_kernel(const RveResi
 #pragma unroll
       for (int c = 0; c < 6; ++c) sig[c] = (T)0;
     }
-    // Element nodal forces w_q B_q^T sigma_q and Jacobi diagonal contributions.
+    // Element nodal forces w_q B_q^T sigma_q and Jacobi diagonal contributions
+    // w e^T C e for the B column e of every (node, direction): e has the node's gradient
+    // component g on the direction's normal strain and the other two components s1, s2 on
+    // its two engineering shears, so with C = K 1(x)1 + f P + c n(x)n
+    //   e^T C e = K g^2 + f (2/3 g^2 + 1/2 (s1^2 + s2^2)) + c (n . e)^2
+    // (elastic: C11 g^2 + G (s1^2 + s2^2)).
     T f[8][3];
     bt_stress(Gr, sig, jw, f);
     T diag[8][3];
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
+      const T gx = Gr.x[b], gy = Gr.y[b], gz = Gr.z[b];
+      // (normal gradient, shear partners, n . e) for directions x, y, z (Voigt xx yy zz yz xz xy)
+      const T gn[3] = {gx, gy, gz};
+      const T sa[3] = {gz, gz, gy}, sb[3] = {gy, gx, gx};
+      const T ne[3] = {tp.n[0] * gx + tp.n[4] * gz + tp.n[5] * gy, tp.n[1] * gy + tp.n[3] * gz + tp.n[5] * gx,
+                       tp.n[2] * gz + tp.n[3] * gy + tp.n[4] * gx};
 #pragma unroll
       for (int dd = 0; dd < 3; ++dd) {
-        T ec[6] = {0, 0, 0, 0, 0, 0};
-        // B column of (node b, direction dd)
-        if (dd == 0) {
-          ec[0] = Gr.x[b];
-          ec[4] = Gr.z[b];
-          ec[5] = Gr.y[b];
-        } else if (dd == 1) {
-          ec[1] = Gr.y[b];
-          ec[3] = Gr.z[b];
-          ec[5] = Gr.x[b];
-        } else {
-          ec[2] = Gr.z[b];
-          ec[3] = Gr.y[b];
-          ec[4] = Gr.x[b];
-        }
-        T sc[6];
-        tangent_apply(m, tp, ec, sc);
-        diag[b][dd] = live ? jw * (ec[0] * sc[0] + ec[1] * sc[1] + ec[2] * sc[2] + ec[3] * sc[3] + ec[4] * sc[4] +
-                                   ec[5] * sc[5])
-                           : (T)0;
+        const T g2 = gn[dd] * gn[dd], s2 = sa[dd] * sa[dd] + sb[dd] * sb[dd];
+        const T v = tp.elastic ? m.C11 * g2 + m.G * s2
+                               : m.K * g2 + tp.f * ((T)(2.0 / 3.0) * g2 + (T)0.5 * s2) + tp.c * ne[dd] * ne[dd];
+        diag[b][dd] = live ? jw * v : (T)0;
       }
     }
     T fo[3], dgo[3];
@@ -415,7 +420,7 @@ __device__ __forceinline__ void gather_node_force(const RveDesc& d, const double
   for (int dd = 0; dd < 3; ++dd) f[dd] = dg[dd] = 0.0;
   for (int n = 0; n < 8; ++n) {
     const int di = n & 1, dj = (n >> 1) & 1, dk = (n >> 2) & 1;
-    const int ie = (i - di + d.nx) % d.nx, je = (j - dj + d.ny) % d.ny, ke = (k - dk + d.nz) % d.nz;
+    const int ie = wrap_down(i - di, d.nx), je = wrap_down(j - dj, d.ny), ke = wrap_down(k - dk, d.nz);
     const int64_t e = d.eoff + ie + (int64_t)d.nx * (je + (int64_t)d.ny * ke);
 #pragma unroll
     for (int dd = 0; dd < 3; ++dd) {
@@ -518,7 +523,7 @@ __device__ double apply_tangent(const RvePcgArgs<T>& a, const RveDesc& d, const 
       const bool live = gl < items;
       const int el = live ? (gl >> 3) : 0;
       const int q = gl & 7;
-      const int i = el % d.nx, j = el / d.nx;
+      const int j = el / d.nx, i = el - j * d.nx;
       const int64_t e = d.eoff + el + (int64_t)nxy * k;
       T mine[3] = {0, 0, 0};
       if (live) {
@@ -556,11 +561,11 @@ __device__ double apply_tangent(const RvePcgArgs<T>& a, const RveDesc& d, const 
     }
     __syncthreads();
     for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
-      const int i = n % d.nx, j = n / d.nx;
+      const int j = n / d.nx, i = n - j * d.nx;
       double bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
       for (int s = 0; s < 4; ++s) {
         const int di = s & 1, dj = s >> 1;
-        const int el = (i - di + d.nx) % d.nx + d.nx * ((j - dj + d.ny) % d.ny);
+        const int el = wrap_down(i - di, d.nx) + d.nx * wrap_down(j - dj, d.ny);
 #pragma unroll
         for (int dd = 0; dd < 3; ++dd) {
           bot[dd] += ye[(8 * el + s) * 3 + dd];
@@ -735,7 +740,7 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
       const bool live = gl < items;
       const int el = live ? (gl >> 3) : 0;
       const int q = gl & 7;
-      const int i = el % d.nx, j = el / d.nx;
+      const int j = el / d.nx, i = el - j * d.nx;
       const int64_t e = d.eoff + el + (int64_t)nxy * k;
       T mine[3] = {0, 0, 0};
       if (live) {
@@ -773,11 +778,11 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
     }
     __syncthreads();
     for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
-      const int i = n % d.nx, j = n / d.nx;
+      const int j = n / d.nx, i = n - j * d.nx;
       double bot[3] = {0, 0, 0}, top[3] = {0, 0, 0};
       for (int s = 0; s < 4; ++s) {
         const int di = s & 1, dj = s >> 1;
-        const int el = (i - di + d.nx) % d.nx + d.nx * ((j - dj + d.ny) % d.ny);
+        const int el = wrap_down(i - di, d.nx) + d.nx * wrap_down(j - dj, d.ny);
 #pragma unroll
         for (int dd = 0; dd < 3; ++dd) {
           bot[dd] += (double)ye[(8 * el + s) * 3 + dd];
@@ -1035,7 +1040,7 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_tangent_rhs_kernel(const RveT
       double f[3] = {0.0, 0.0, 0.0};
       for (int n = 0; n < 8; ++n) {
         const int di = n & 1, dj = (n >> 1) & 1, dk = (n >> 2) & 1;
-        const int ie = (i - di + d.nx) % d.nx, je = (j - dj + d.ny) % d.ny, ke = (k - dk + d.nz) % d.nz;
+        const int ie = wrap_down(i - di, d.nx), je = wrap_down(j - dj, d.ny), ke = wrap_down(k - dk, d.nz);
         const int64_t e = d.eoff + ie + (int64_t)d.nx * (je + (int64_t)d.ny * ke);
 #pragma unroll
         for (int dd = 0; dd < 3; ++dd) f[dd] += a.fe6[((int64_t)jcol * a.ne_total * 8 + 8 * e + n) * 3 + dd];
@@ -1322,7 +1327,7 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_response_kernel(const RveResp
     const double* eb = a.macro + 6 * r;
     const double ua[3] = {x * eb[0] + 0.5 * z * eb[4] + 0.5 * y * eb[5], y * eb[1] + 0.5 * z * eb[3] + 0.5 * x * eb[5],
                           z * eb[2] + 0.5 * y * eb[3] + 0.5 * x * eb[4]};
-    const double xr = (I % d.nx) * d.hx, yr = (J % d.ny) * d.hy, zr = (K % d.nz) * d.hz;
+    const double xr = wrap_up(I, d.nx) * d.hx, yr = wrap_up(J, d.ny) * d.hy, zr = wrap_up(K, d.nz) * d.hz;
     const double ur[3] = {xr * eb[0] + 0.5 * zr * eb[4] + 0.5 * yr * eb[5],
                           yr * eb[1] + 0.5 * zr * eb[3] + 0.5 * xr * eb[5],
                           zr * eb[2] + 0.5 * yr * eb[3] + 0.5 * xr * eb[4]};
