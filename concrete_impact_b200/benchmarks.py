@@ -408,6 +408,75 @@ def fe2_accuracy(rno, envelope, steps: int = 400, divisions=(64, 2, 2), precisio
             "stress_rms_pa": float(s_ref.pow(2).mean().sqrt().item())}  # fmt: skip
 
 
+def fe2_closed_loop(rno, envelope, steps: int = 400, divisions=(64, 16, 16), fallback_capacity: int = 32768) -> dict:
+    """Surrogate FE^2 against all-direct FE^2 (FP32 RVEs; FP64 RVEs of all 131,072 points do
+    not fit in HBM) on the full bar over ``steps`` steps from rest: relative Frobenius
+    errors of the macro stress and displacement histories (closed loop), and of the
+    surrogate alone along the direct run's strain histories (open loop)."""
+    from .fe2 import DirectRVEPoints, ExplicitFE2, RNOPoints, build_macro_bar, stable_time_step
+    from .rno import RNODataset
+    from .rno_data import relative_stress_error
+
+    model32 = concrete_rve(8, 0, 32)
+    lengths = tuple(0.01 * d for d in divisions)
+    bar = build_macro_bar(divisions, lengths, 2400.0)
+    dt = stable_time_step(bar, model32.material.maximum_wave_speed, 0.5)
+    t0 = time.perf_counter()
+    direct = ExplicitFE2(bar, DirectRVEPoints(model32, bar.points, UPDATE_SETTINGS, precision=32), dt)
+    s_ref, u_ref, e_ref = _record_run(direct, steps)
+    del direct
+    torch.cuda.empty_cache()
+    direct_s = time.perf_counter() - t0
+    zeros = torch.zeros((bar.points, 1, 6), dtype=torch.float64, device=e_ref.device)
+    paths = RNODataset(torch.cat([zeros, e_ref.transpose(0, 1)], dim=1), torch.cat([zeros, s_ref.transpose(0, 1)], dim=1),
+                       torch.full((bar.points, steps), dt, dtype=torch.float64, device=e_ref.device))  # fmt: skip
+    open_loop = relative_stress_error(rno.rollout(paths), paths.stress[:, 1:])
+    del paths
+    gate = RNOPoints(rno, bar.points, envelope, model32, UPDATE_SETTINGS, fallback_capacity=fallback_capacity)
+    surrogate = ExplicitFE2(bar, gate, dt)
+    s_rno, u_rno, _ = _record_run(surrogate, steps)
+    out = {"steps": steps, "divisions": list(divisions), "dt": dt, "points": bar.points,
+           "homogenised_stress_error_open_loop": open_loop,
+           "stress_error": relative_stress_error(s_rno, s_ref), "displacement_error": relative_stress_error(u_rno, u_ref),
+           "flagged_points": int(gate.slots_used), "direct_reference": "all-direct FE2, FP32 8^3 RVEs",
+           "direct_run_s": direct_s, "stress_rms_pa": float(s_ref.pow(2).mean().sqrt().item())}  # fmt: skip
+    del surrogate, gate, s_ref, u_ref, e_ref, s_rno, u_rno
+    torch.cuda.empty_cache()
+    return out
+
+
+def fe2_judged(rno, envelope, steps: int = 5000, warmup: int = 5, divisions=(64, 16, 16), sample: int = 256,
+               every: int = 1, threshold: float = 0.05, fallback_capacity: int = 32768, seed: int = 0) -> dict:  # fmt: skip
+    """Surrogate FE^2 on the full bar with the runtime judge (``SurrogateJudge``: FP64
+    direct RVEs at ``sample`` seeded macro points, every ``every`` steps): macro steps/s
+    with the judge's cost included, the judged homogenised-stress error over the run and
+    the escalations to the fallback pool."""
+    from .fe2 import ExplicitFE2, RNOPoints, SurrogateJudge, build_macro_bar, stable_time_step
+
+    model32 = concrete_rve(8, 0, 32)
+    lengths = tuple(0.01 * d for d in divisions)
+    bar = build_macro_bar(divisions, lengths, 2400.0)
+    dt = stable_time_step(bar, model32.material.maximum_wave_speed, 0.5)
+    judge = SurrogateJudge(concrete_rve(8, 0, 64), bar.points, UPDATE_SETTINGS, sample=sample, every=every,
+                           threshold=threshold, seed=seed)  # fmt: skip
+    gate = RNOPoints(rno, bar.points, envelope, model32, UPDATE_SETTINGS, fallback_capacity=fallback_capacity,
+                     judge=judge)  # fmt: skip
+    fe2 = ExplicitFE2(bar, gate, dt)
+    fe2.run(warmup)
+    ms = _elapsed_ms(lambda: fe2.run(steps))
+    hist = judge.history
+    picks = sorted({0, len(hist) // 4, len(hist) // 2, 3 * len(hist) // 4, len(hist) - 1}) if hist else []
+    out = {"steps": steps, "ms": ms, "steps_per_s": steps / (ms / 1e3), "sample": int(judge.points.numel()),
+           "every": every, "threshold": threshold, "judge_steps": judge.judge_steps, "judged_error": judge.error,
+           "worst_point_error": max((h[2] for h in hist), default=0.0), "escalations": gate.escalations,
+           "flagged_points": int(gate.slots_used),
+           "history": [{"step": hist[i][0], "error": hist[i][1], "worst_point": hist[i][2]} for i in picks],
+           "judge_precision": "FP64 direct 8^3 RVEs (the reference's precision)"}  # fmt: skip
+    del fe2, gate, judge
+    torch.cuda.empty_cache()
+    return out
+
+
 def fe2_speed(rno, envelope, rno_steps: int = 5000, rno_warmup: int = 5, direct_steps: int = 3,
               divisions=(64, 16, 16), fallback_capacity: int = 32768, time_limit_s: float = 180.0) -> dict:  # fmt: skip
     """Macro steps/s of surrogate FE^2 (``rno_steps`` steps) and of all-direct FE^2 (FP32 RVEs,

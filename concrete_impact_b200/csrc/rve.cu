@@ -73,6 +73,35 @@ __device__ __forceinline__ void physical_grads(int q, const RveDesc& d, Grad8<T>
   }
 }
 
+// The gradients of all 8 Gauss points of a box element in shared memory, entry (a, d) of
+// point q at tab[(3 a + d) * 8 + q]: the lanes of a warp that share q read the same word.
+// The PCG kernels fill it once per solve (one RVE per system; a thread's Gauss point is
+// fixed because the item stride is a multiple of 8) instead of forming the gradients for
+// every element of every CG iteration.
+template <typename T>
+__device__ __forceinline__ void fill_grad_table(const RveDesc& d, T* tab) {
+  if (threadIdx.x < 8) {
+    Grad8<T> G;
+    physical_grads((int)threadIdx.x, d, G);
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      tab[(3 * a + 0) * 8 + threadIdx.x] = G.x[a];
+      tab[(3 * a + 1) * 8 + threadIdx.x] = G.y[a];
+      tab[(3 * a + 2) * 8 + threadIdx.x] = G.z[a];
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void load_grads(const T* tab, int q, Grad8<T>& G) {
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    G.x[a] = tab[(3 * a + 0) * 8 + q];
+    G.y[a] = tab[(3 * a + 1) * 8 + q];
+    G.z[a] = tab[(3 * a + 2) * 8 + q];
+  }
+}
+
 // eps = B u for the 24 nodal values u[a][d] (Voigt xx,yy,zz,yz,xz,xy; engineering shear).
 template <typename T>
 __device__ __forceinline__ void strain_from(const Grad8<T>& G, const T u[8][3], T e[6]) {
@@ -507,7 +536,7 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_gather_norms_kernel(const Rve
 // gathers its 4 bottom and 4 top contributions in a fixed order.  Returns p . Ap (CTA-wide).
 template <typename T>
 __device__ double apply_tangent(const RvePcgArgs<T>& a, const RveDesc& d, const double* __restrict__ p,
-                                double* __restrict__ Ap, double* smem, double* scratch) {
+                                double* __restrict__ Ap, double* smem, double* scratch, const T* gtab) {
   const int nxy = d.nx * d.ny;
   double* ye = smem;                  // nxy * 24
   double* acc_cur = ye + 24 * nxy;    // nxy * 3
@@ -534,7 +563,7 @@ __device__ double apply_tangent(const RvePcgArgs<T>& a, const RveDesc& d, const 
       T u[8][3];
       allgather8(mine, u);
       Grad8<T> Gr;
-      physical_grads(q, d, Gr);
+      load_grads(gtab, q, Gr);
       T eps[6], sig[6];
       strain_from(Gr, u, eps);
       const int64_t g = 8 * e + q;
@@ -637,6 +666,8 @@ __global__ void __launch_bounds__(RVE_THREADS, 2) rve_pcg_kernel(const RvePcgArg
   double* p = a.p + off;
   double* Ap = a.Ap + off;
   const double* dinv = a.dinv + 3 * d.eoff;
+  __shared__ T gtab[24 * 8];
+  fill_grad_table(d, gtab);  // visible after the block sum below
   // Shift the vector pointers so that batch node indices address them directly.
   const int64_t shift = 3 * d.eoff;
   double* x_ = x - shift;
@@ -663,7 +694,7 @@ __global__ void __launch_bounds__(RVE_THREADS, 2) rve_pcg_kernel(const RvePcgArg
     status = (bnorm == 0.0) ? 0 : 2;
   } else {
     for (iters = 0; iters < a.maxit;) {
-      const double pap = apply_tangent<T>(a, d, p_, Ap_, smem, scratch);
+      const double pap = apply_tangent<T>(a, d, p_, Ap_, smem, scratch, gtab);
       if (!(pap > 0.0) || !isfinite(pap)) {
         status = 2;
         break;
@@ -723,7 +754,8 @@ __global__ void __launch_bounds__(RVE_THREADS, 2) rve_pcg_kernel(const RvePcgArg
 template <typename T>
 __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, const double* __restrict__ p,
                                      double* __restrict__ Ap, unsigned char* smem, int k0, int k1,
-                                     cg::cluster_group& cl, unsigned prev_rank) {
+                                     cg::cluster_group& cl, unsigned prev_rank,
+                                     const T* gtab) {
   const int nxy = d.nx * d.ny;
   T* ye = reinterpret_cast<T*>(smem);  // nxy * 24 element-node contributions of one layer (exact in T)
   double* acc_cur = reinterpret_cast<double*>(smem + (size_t)24 * nxy * sizeof(T));  // nxy * 3 node sums
@@ -751,7 +783,7 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
       T u[8][3];
       allgather8(mine, u);
       Grad8<T> Gr;
-      physical_grads(q, d, Gr);
+      load_grads(gtab, q, Gr);
       T eps[6], sig[6];
       strain_from(Gr, u, eps);
       const int64_t g = 8 * e + q;
@@ -896,6 +928,8 @@ __global__ void __launch_bounds__(PcgShape<T, SHAPE>::threads, PcgShape<T, SHAPE
     return;
   }
   const int nxy = d.nx * d.ny;
+  __shared__ T gtab[24 * 8];
+  fill_grad_table(d, gtab);  // visible after the first cluster sum
   const int k0 = (int)((rank * (unsigned)d.nz) / C), k1 = (int)(((rank + 1) * (unsigned)d.nz) / C);
   const unsigned prev_rank = (rank + C - 1) % C;
   const int64_t off = a.sys_off[s];
@@ -927,7 +961,7 @@ __global__ void __launch_bounds__(PcgShape<T, SHAPE>::threads, PcgShape<T, SHAPE
     status = (bnorm == 0.0) ? 0 : 2;
   } else {
     for (iters = 0; iters < a.maxit;) {
-      double pap[1] = {apply_tangent_slab<T>(a, d, p - shift, Ap - shift, smem, k0, k1, cl, prev_rank)};
+      double pap[1] = {apply_tangent_slab<T>(a, d, p - shift, Ap - shift, smem, k0, k1, cl, prev_rank, gtab)};
       cluster_sum<1>(pap, scratch, slot_pap, cl);
       if (!(pap[0] > 0.0) || !isfinite(pap[0])) {
         status = 2;

@@ -13,7 +13,11 @@ pressure (src/fem/assembly/load.py:40-77), with the macro kernels of ``csrc/hex8
 * ``RNOPoints`` -- the recurrent surrogate with one latent state per point, behind an error
   gate: a point whose surrogate input leaves the training envelope falls back to a direct
   RVE solve (fallback pool of RVEs; its RVE starts with a catch-up step that loads it
-  proportionally to the current macro strain over the elapsed time).
+  proportionally to the current macro strain over the elapsed time), and optionally a
+  runtime judge (``SurrogateJudge``): direct FP64 RVEs at a seeded sample of points follow
+  the run's macro strains, measure the error of the delivered stress against the direct
+  solve, and escalate a sampled point whose error passes a threshold to the fallback pool
+  with its direct RVE history.
 """
 
 from __future__ import annotations
@@ -128,7 +132,7 @@ class DirectRVEPoints:
         self.model = model
         self.n = n_points
         self.settings = update_settings
-        self.batches = [RVEBatch([model] * min(chunk, n_points - s), precision=precision)
+        self.batches = [RVEBatch([model] * min(chunk, n_points - s), precision=precision, device_control=True)
                         for s in range(0, n_points, chunk)]  # fmt: skip
         self.starts = list(range(0, n_points, chunk))
         self.volume = float(self.batches[0].volumes[0])
@@ -151,6 +155,80 @@ class DirectRVEPoints:
             b.commit()
 
 
+class SurrogateJudge:
+    """Direct RVE solves that judge the surrogate's error during an FE^2 run.
+
+    A seeded sample of ``sample`` macro points carries its own direct RVEs (``precision``
+    64: the reference's precision), advanced along the surrogate run's macro strains every
+    ``every`` macro steps (one RVE step over the elapsed interval).  At each judge step the
+    stress delivered at those points (surrogate, or fallback where a point was flagged) is
+    compared with the direct homogenised stress; the judge keeps the squared errors and
+    squared reference stresses per point, so ``error`` is the relative Frobenius error of
+    the homogenised stress over the sampled points and judge steps.  A sampled point whose
+    own relative error exceeds ``threshold`` (once its reference stress exceeds
+    ``stress_floor``) is escalated: it leaves the surrogate for the fallback pool, which
+    takes over the judge's RVE state of that point (its exact history).  One host read per
+    judge step decides the escalations.
+    """
+
+    def __init__(self, model: StructuredHex8RVE, n_points: int, update_settings: MaterialUpdateSettings,
+                 sample: int = 256, every: int = 1, threshold: float = 0.05, stress_floor: float = 1.0e6,
+                 seed: int = 0, precision: int = 64) -> None:  # fmt: skip
+        rng = np.random.default_rng(seed)
+        pts = np.sort(rng.choice(n_points, size=min(sample, n_points), replace=False))
+        self.model = model
+        self.settings = update_settings
+        self.every = max(int(every), 1)
+        self.threshold = float(threshold)
+        self.floor2 = float(stress_floor) ** 2
+        self.batch = RVEBatch([model] * pts.size, precision=precision, device_control=True)
+        dev = self.batch.device
+        self.points = torch.as_tensor(pts, device=dev)
+        self.volume = float(self.batch.volumes[0])
+        self.sq_err = torch.zeros(pts.size, dtype=torch.float64, device=dev)
+        self.sq_ref = torch.zeros(pts.size, dtype=torch.float64, device=dev)
+        self.escalated = torch.zeros(pts.size, dtype=torch.bool, device=dev)
+        self.count = 0
+        self.elapsed = 0.0
+        self.judge_steps = 0
+        self.history: list[tuple[int, float, float]] = []  # (macro step, running error, worst point error)
+
+    @property
+    def error(self) -> float:
+        ref = float(self.sq_ref.sum())
+        return math.sqrt(float(self.sq_err.sum()) / ref) if ref > 0.0 else 0.0
+
+    def observe(self, strain: torch.Tensor, delivered: torch.Tensor, dt: float) -> torch.Tensor | None:
+        """After a macro step's material update: every ``every`` steps solve the sampled
+        RVEs and compare.  Returns the sample slots to escalate (or None)."""
+        self.count += 1
+        self.elapsed += dt
+        if self.count % self.every:
+            return None
+        b = self.batch
+        b.macro.copy_(strain[self.points])
+        b.dt.fill_(self.elapsed)
+        self.elapsed = 0.0
+        solve_batch_step(b, self.model.newton_settings, self.settings, False)
+        b.response(b.batch_struct(self.settings), b.w, None, None)
+        ref = b.sums[:, RS_SIGMA : RS_SIGMA + 6] / self.volume
+        b.commit()
+        self.reference = ref
+        diff = delivered[self.points] - ref
+        self.sq_err += (diff * diff).sum(dim=1)
+        self.sq_ref += (ref * ref).sum(dim=1)
+        self.judge_steps += 1
+        point_err2 = self.sq_err / self.sq_ref.clamp(min=1e-300)
+        bad = (point_err2 > self.threshold**2) & (self.sq_ref > self.floor2 * self.judge_steps) & ~self.escalated
+        worst = float(point_err2.max().sqrt())
+        self.history.append((self.count, self.error, worst))
+        slots = torch.nonzero(bad).flatten()
+        if slots.numel() == 0:
+            return None
+        self.escalated[slots] = True
+        return slots
+
+
 class RNOPoints:
     """The surrogate at every macro point, with an input-envelope gate and a direct fallback.
 
@@ -163,8 +241,11 @@ class RNOPoints:
 
     def __init__(self, rno: RNOSurrogate, n_points: int, envelope: tuple[float, float],
                  model: StructuredHex8RVE | None = None, update_settings: MaterialUpdateSettings | None = None,
-                 envelope_factor: float = 1.05, fallback_capacity: int = 2048, precision: int = 32) -> None:  # fmt: skip
+                 envelope_factor: float = 1.05, fallback_capacity: int = 2048, precision: int = 32,
+                 judge: SurrogateJudge | None = None) -> None:  # fmt: skip
         self.rno = rno
+        self.judge = judge
+        self.escalations = 0
         self.n = n_points
         dev = rno.device
         self.z = torch.zeros((n_points, 6), dtype=torch.float32, device=dev)
@@ -178,7 +259,8 @@ class RNOPoints:
         self.flagged = torch.zeros(n_points, dtype=torch.bool, device=dev)
         self.slot_of = torch.full((n_points,), -1, dtype=torch.int64, device=dev)
         self.slots_used = 0
-        self.pool = RVEBatch([model] * fallback_capacity, precision=precision) if model is not None else None
+        self.pool = (RVEBatch([model] * fallback_capacity, precision=precision, device_control=True)
+                     if model is not None else None)  # fmt: skip
         self.capacity = fallback_capacity if model is not None else 0
         self.pool_points = torch.full((self.capacity,), -1, dtype=torch.int64, device=dev)
         self.time = 0.0
@@ -198,6 +280,52 @@ class RNOPoints:
             self.count = torch.zeros(1, dtype=torch.int32, device=dev)
 
     def stress(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
+        stress = self._stress(strain, rate, dt)
+        if self.judge is not None:
+            slots = self.judge.observe(strain, stress, dt)
+            if slots is not None:
+                stress = stress.clone()
+                self._escalate(slots, stress)
+        return stress
+
+    def _escalate(self, slots: torch.Tensor, stress: torch.Tensor) -> None:
+        """Move judged points whose error passed the threshold to the fallback pool with
+        the judge's RVE state; their stress of this step is the judge's."""
+        judge = self.judge
+        pts = judge.points[slots]
+        keep = ~self.flagged[pts]
+        slots, pts = slots[keep], pts[keep]
+        if pts.numel() == 0:
+            return
+        room = self.capacity - self.slots_used
+        if pts.numel() > room:
+            raise RuntimeError(f"the judge escalated more points than the fallback pool holds ({self.capacity}).")
+        a, b = self.slots_used, self.slots_used + int(pts.numel())
+        p, j = self.pool, judge.batch
+        E = int(p.elem_counts[0])
+        for k, (slot, pt) in enumerate(zip(range(a, b), slots.tolist())):
+            g0, g1, h0, h1 = 8 * E * slot, 8 * E * (slot + 1), 8 * E * pt, 8 * E * (pt + 1)
+            # committed and trial state alike: the step's commit copies trial -> committed
+            for dst, src in ((p.ep_n, j.ep_n), (p.ep, j.ep_n)):
+                dst[:, g0:g1] = src[:, h0:h1].to(dst.dtype)
+            for dst in (p.q_n, p.q):
+                dst[g0:g1] = j.q_n[h0:h1]
+            for dst in (p.vpm_n, p.vpm):
+                dst[g0:g1] = j.vpm_n[h0:h1]
+            for dst in (p.w_n, p.w):
+                dst[3 * E * slot : 3 * E * (slot + 1)] = j.w_n[3 * E * pt : 3 * E * (pt + 1)]
+            p.macro_n[slot] = j.macro_n[pt]
+            p.macro[slot] = j.macro_n[pt]
+        self.pool_points[a:b] = pts
+        self.flagged[pts] = True
+        if self.rno.fused:
+            self.flag8[pts] = 1
+        self.slot_of[pts] = torch.arange(a, b, device=pts.device)
+        self.slots_used = b
+        stress[pts] = judge.reference[slots]
+        self.escalations += int(pts.numel())
+
+    def _stress(self, strain: torch.Tensor, rate: torch.Tensor, dt: float) -> torch.Tensor:
         if self.rno.fused and self.pool is not None:
             return self._stress_fused(strain, rate, dt)
         s = self.rno.scales

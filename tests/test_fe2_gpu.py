@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 
 from concrete_impact_b200 import _native  # noqa: E402
 from concrete_impact_b200.fe2 import (  # noqa: E402
+    SurrogateJudge,
     DirectRVEPoints,
     ExplicitFE2,
     MaterialPoints,
@@ -222,3 +223,50 @@ def test_generated_paths_of_single_phase_rve_match_point_law() -> None:
     np.testing.assert_allclose(data.strain.cpu().numpy(), strains)
     env = input_envelope(RNOScales(1e-3, 10.0, 1e7), data)
     assert env[0] > 0 and env[1] > 0
+
+
+def test_judge_measures_the_delivered_stress_against_direct_rves() -> None:
+    """The runtime judge's RVEs follow the sampled points' macro strains: with every point
+    flagged to the (FP64) fallback pool the delivered stress is the direct one, so the
+    judged error is at roundoff; with a huge envelope the untrained surrogate delivers, and
+    the judge reports its error (the same relative Frobenius error as the delivered stress
+    against independent direct RVEs at those points) and escalates the worst points, whose
+    answers are the direct ones from then on."""
+    div, lengths = (4, 1, 1), (0.04, 0.01, 0.01)
+    bar = build_macro_bar(div, lengths, 2400.0)
+    dt = stable_time_step(bar, MORTAR.maximum_wave_speed, 0.5)
+    rve = build_structured_rve((2, 2, 2), MORTAR, default_newton())
+    steps, pulse = 10, _pulse(16 * dt)
+    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=1e9, stress_floor=0.0, seed=3)
+    gated = RNOPoints(_untrained_rno(), bar.points, (-1.0, -1.0), rve, SETTINGS, fallback_capacity=bar.points,
+                      precision=64, judge=judge)  # fmt: skip
+    ExplicitFE2(bar, gated, dt, pulse).run(steps)
+    assert judge.judge_steps == steps and judge.error < 1e-10
+    # surrogate answers, judged against independent direct RVEs along the same histories
+    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=1e9, stress_floor=0.0, seed=3)
+    free = RNOPoints(_untrained_rno(), bar.points, (1e30, 1e30), rve, SETTINGS, fallback_capacity=bar.points,
+                     precision=64, judge=judge)  # fmt: skip
+    fe2 = ExplicitFE2(bar, free, dt, pulse)
+    shadow = DirectRVEPoints(rve, int(judge.points.numel()), SETTINGS, precision=64)
+    err2 = ref2 = 0.0
+    for _ in range(steps):
+        fe2.step()
+        direct = shadow.stress(fe2.strain[judge.points], fe2.rate[judge.points], dt)
+        shadow.commit()
+        d = fe2.last_stress[judge.points] - direct
+        err2 += float((d * d).sum())
+        ref2 += float((direct * direct).sum())
+    assert judge.error == pytest.approx((err2 / ref2) ** 0.5, rel=1e-9)
+    assert judge.error > 0.05 and free.escalations == 0
+    # a threshold below that error escalates the sampled points to the fallback pool
+    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=0.05, stress_floor=0.0, seed=3)
+    esc = RNOPoints(_untrained_rno(), bar.points, (1e30, 1e30), rve, SETTINGS, fallback_capacity=bar.points,
+                    precision=64, judge=judge)  # fmt: skip
+    fe2 = ExplicitFE2(bar, esc, dt, pulse)
+    fe2.run(steps)
+    assert esc.escalations > 0 and esc.slots_used == esc.escalations
+    escalated = judge.points[judge.escalated]
+    assert bool(esc.flagged[escalated].all())
+    # escalated points carry the judge's RVE history: their answers equal the judge's
+    fe2.step()
+    torch.testing.assert_close(fe2.last_stress[escalated], judge.reference[judge.escalated], rtol=1e-9, atol=1e-3)
