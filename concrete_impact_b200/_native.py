@@ -234,6 +234,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "cib_energy_rno_param_count": (_I64, [ctypes.c_int32] * 3),
     "cib_energy_rno_anchors": (_I, [_P, _P, _P]),
     "cib_energy_rno_update": (_I, [_P, _I64] + [_P] * 10),
+    "cib_energy_rno_tangent": (_I, [_P, _I64] + [_P] * 5),
     "cib_newmark_kinematics": (_I, [_I64, _P, _P, _P, _D, _D, _P, _P, _P]),
     "cib_newmark_residual": (_I, [_I64] + [_P] * 9),
     "cib_newmark_effective_tangent": (_I, [_I64, _P, _P, _P, _P, _D, _P, _P, _P, _P]),

@@ -238,6 +238,7 @@ struct EnergyArgs {
   float* rate_dimless;      // n x L
   float* scalars;           // 4 x n: dissipation, free energy, violation, energy increment
   float* anchors_out;       // anchor mode: 14 outputs (point 0 of a zero input)
+  float* tangent;           // tangent kernel: n x 6 x 6
 };
 
 __global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs a) {
@@ -368,6 +369,284 @@ __global__ void __launch_bounds__(ER_THREADS) energy_rno_kernel(const EnergyArgs
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Algorithmic tangent d stress / d strain (the reference differentiates the stress with
+// autograd, rve_rno.py:283-297).  With network strain e^ = strain / scale,
+//   stress_i = (dW_eq/de^_i (e^) + dW_neq/de^_i (e^, z*)) / s_i  (+ constants)
+// where z* is the candidate latent z + (dt / tau) f(e^, z) of the current-state integrator
+// (the previous latent for the other integrator, which does not depend on the strain), so
+//   C_ij = (H_eq(e^)_ij + [H_neq(e^, z*) v_j]_i) / (s_i s_j),  v_j = (e_j, (dt / tau) J_f e_j)
+// with J_f the strain Jacobian of the evolution network.  Every Hessian-vector product is
+// a forward-over-reverse pass of a SiLU MLP y = w_o . h_{L-1}, h_l = silu(a_l),
+// a_l = W_l h_{l-1} + b_l:
+//   primal:   a_l (kept), g_{L-1} = w_o, g_{l-1} = W_l^T (g_l * silu'(a_l)) (kept)
+//   forward:  adot_0 = W_0 v, adot_l = W_l (silu'(a_{l-1}) * adot_{l-1}) (kept)
+//   backward: ddot_{L-1} = w_o * silu''(a_{L-1}) adot_{L-1},
+//             ddot_l = (W_{l+1}^T ddot_{l+1}) * silu'(a_l) + g_l * silu''(a_l) adot_l,
+//             H v = W_0^T ddot_0.
+// One CTA of 128 threads per tile of 32 points, the same feature-major shared layout as
+// the update kernel; the tangent directions are looped (6 per network).
+
+__device__ __forceinline__ float silu_second(float z) {
+  const float s = 1.0f / (1.0f + expf(-z));
+  return s * (1.0f - s) * (2.0f + z * (1.0f - 2.0f * s));
+}
+
+struct TanSmem {
+  float* x;    // [XLD][TILE] primal input, then the tangent direction
+  float* gin;  // [XLD][TILE] input gradient / Hessian-vector product
+  float* h0;   // [hidden][TILE] work
+  float* h1;   // [hidden][TILE] work
+  float* z;    // [layers][hidden][TILE] pre-activations a_l
+  float* ad;   // [layers][hidden][TILE] tangent pre-activations adot_l
+  float* g;    // [layers - 1][hidden][TILE] activation gradients g_l, l < L - 1
+};
+
+// out[j][p] = sum_k W_l[j][k] in[k][p] (+ b_j), thread j < hidden (weights read transposed).
+__device__ void tan_mat_forward(const float* Wt, const float* b, int in_l, int hidden, const float* in, float* out) {
+  const int j = threadIdx.x;
+  if (j < hidden) {
+    float acc[ER_TILE];
+    const float bj = b ? b[j] : 0.0f;
+#pragma unroll
+    for (int p = 0; p < ER_TILE; ++p) acc[p] = bj;
+    for (int k = 0; k < in_l; ++k) {
+      const float w = Wt[(int64_t)k * hidden + j];
+#pragma unroll
+      for (int q = 0; q < ER_TILE / 4; ++q) {
+        const float4 v = *grp(in, k, q);
+        acc[4 * q] = fmaf(w, v.x, acc[4 * q]);
+        acc[4 * q + 1] = fmaf(w, v.y, acc[4 * q + 1]);
+        acc[4 * q + 2] = fmaf(w, v.z, acc[4 * q + 2]);
+        acc[4 * q + 3] = fmaf(w, v.w, acc[4 * q + 3]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < ER_TILE / 4; ++q)
+      *grp(out, j, q) = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+  }
+  __syncthreads();
+}
+
+// out[t][p] = sum_j W_l[j][t] d[j][p], thread t < in_l.
+__device__ void tan_mat_backward(const float* W, int in_l, int hidden, const float* d, float* out) {
+  const int t = threadIdx.x;
+  if (t < in_l) {
+    float acc[ER_TILE];
+#pragma unroll
+    for (int p = 0; p < ER_TILE; ++p) acc[p] = 0.0f;
+    for (int j = 0; j < hidden; ++j) {
+      const float w = W[(int64_t)j * in_l + t];
+#pragma unroll
+      for (int q = 0; q < ER_TILE / 4; ++q) {
+        const float4 v = *grp(d, j, q);
+        acc[4 * q] = fmaf(v.x, w, acc[4 * q]);
+        acc[4 * q + 1] = fmaf(v.y, w, acc[4 * q + 1]);
+        acc[4 * q + 2] = fmaf(v.z, w, acc[4 * q + 2]);
+        acc[4 * q + 3] = fmaf(v.w, w, acc[4 * q + 3]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < ER_TILE / 4; ++q)
+      *grp(out, t, q) = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
+  }
+  __syncthreads();
+}
+
+// Elementwise over a [hidden][TILE] buffer (thread j owns row j).
+template <typename F>
+__device__ __forceinline__ void tan_rows(int hidden, F f) {
+  const int j = threadIdx.x;
+  if (j < hidden)
+#pragma unroll
+    for (int p = 0; p < ER_TILE; ++p) f(j, p);
+  __syncthreads();
+}
+
+// Primal forward (a_l kept) and backward (g_l kept) of a network at the input in s.x;
+// returns the buffer of the last activation h_{L-1} (for the output layer).
+__device__ const float* tan_primal(const NetView& n, int hidden, int layers, const TanSmem& s, bool backward) {
+  const float* hin = s.x;
+  float* hout = s.h0;
+  for (int l = 0; l < layers; ++l) {
+    const float *W, *Wt, *b;
+    layer_ptrs(n, hidden, l, &W, &Wt, &b);
+    float* zl = s.z + (int64_t)l * hidden * ER_TILE;
+    tan_mat_forward(Wt, b, l == 0 ? n.in : hidden, hidden, hin, zl);
+    tan_rows(hidden, [&](int j, int p) { hout[sw(j, p)] = silu(zl[sw(j, p)]); });
+    hin = hout;
+    hout = (hout == s.h0) ? s.h1 : s.h0;
+  }
+  const float* last = hin;
+  if (!backward) return last;
+  const float* wo = output_ptr(n, hidden, layers);
+  // g_{L-1} = w_o; d = g * silu'(a); g_{l-1} = W_l^T d
+  float* d = (last == s.h0) ? s.h1 : s.h0;  // keep h_{L-1} intact
+  for (int l = layers - 1; l >= 1; --l) {
+    const float* zl = s.z + (int64_t)l * hidden * ER_TILE;
+    const float* gl = l == layers - 1 ? nullptr : s.g + (int64_t)l * hidden * ER_TILE;
+    tan_rows(hidden, [&](int j, int p) {
+      const float gv = gl ? gl[sw(j, p)] : wo[j];
+      d[sw(j, p)] = gv * silu_prime(zl[sw(j, p)]);
+    });
+    const float *W, *Wt, *b;
+    layer_ptrs(n, hidden, l, &W, &Wt, &b);
+    tan_mat_backward(W, hidden, hidden, d, s.g + (int64_t)(l - 1) * hidden * ER_TILE);
+  }
+  return last;
+}
+
+// Forward tangent from the direction in s.x: adot_l kept in s.ad; returns the buffer of
+// hdot_{L-1} = silu'(a_{L-1}) adot_{L-1}.
+__device__ const float* tan_forward(const NetView& n, int hidden, int layers, const TanSmem& s) {
+  const float* in = s.x;
+  float* hd = s.h0;
+  for (int l = 0; l < layers; ++l) {
+    const float *W, *Wt, *b;
+    layer_ptrs(n, hidden, l, &W, &Wt, &b);
+    float* adl = s.ad + (int64_t)l * hidden * ER_TILE;
+    tan_mat_forward(Wt, nullptr, l == 0 ? n.in : hidden, hidden, in, adl);
+    const float* zl = s.z + (int64_t)l * hidden * ER_TILE;
+    tan_rows(hidden, [&](int j, int p) { hd[sw(j, p)] = silu_prime(zl[sw(j, p)]) * adl[sw(j, p)]; });
+    in = hd;
+    hd = (hd == s.h0) ? s.h1 : s.h0;
+  }
+  return in;
+}
+
+// Backward tangent after tan_forward: H v into rows 0..in of s.gin.
+__device__ void tan_backward(const NetView& n, int hidden, int layers, const TanSmem& s) {
+  const float* wo = output_ptr(n, hidden, layers);
+  float* gd = s.h0;  // W_{l+1}^T ddot_{l+1}
+  float* dd = s.h1;  // ddot_l
+  for (int l = layers - 1; l >= 0; --l) {
+    const float* zl = s.z + (int64_t)l * hidden * ER_TILE;
+    const float* adl = s.ad + (int64_t)l * hidden * ER_TILE;
+    const float* gl = l == layers - 1 ? nullptr : s.g + (int64_t)l * hidden * ER_TILE;
+    tan_rows(hidden, [&](int j, int p) {
+      const float z = zl[sw(j, p)];
+      const float second = (gl ? gl[sw(j, p)] : wo[j]) * silu_second(z) * adl[sw(j, p)];
+      dd[sw(j, p)] = (gl ? gd[sw(j, p)] * silu_prime(z) : 0.0f) + second;
+    });
+    const float *W, *Wt, *b;
+    layer_ptrs(n, hidden, l, &W, &Wt, &b);
+    tan_mat_backward(W, l == 0 ? n.in : hidden, hidden, dd, l == 0 ? s.gin : gd);
+  }
+}
+
+__global__ void __launch_bounds__(ER_THREADS) energy_rno_tangent_kernel(const EnergyArgs a) {
+  extern __shared__ float sm[];
+  const int hidden = a.hidden, layers = a.layers, L = a.latent;
+  TanSmem s;
+  s.x = sm;
+  s.gin = s.x + ER_TILE * ER_XLD;
+  s.h0 = s.gin + ER_TILE * ER_XLD;
+  s.h1 = s.h0 + ER_TILE * hidden;
+  s.z = s.h1 + ER_TILE * hidden;
+  s.ad = s.z + (int64_t)layers * ER_TILE * hidden;
+  s.g = s.ad + (int64_t)layers * ER_TILE * hidden;
+  float* eps = s.g + (int64_t)(layers - 1) * ER_TILE * hidden;  // [TILE][6] network strain
+  float* zin = eps + ER_TILE * 6;                                // [TILE][8] previous latent
+  float* zc = zin + ER_TILE * 8;                                 // [TILE][8] candidate latent
+  float* jf = zc + ER_TILE * 8;                                  // [TILE][8][6] (dt / tau) J_f
+  float* cdt = jf + ER_TILE * 48;                                // [TILE] dt / tau
+  const int t = threadIdx.x;
+  const int64_t p0 = (int64_t)blockIdx.x * ER_TILE;
+  const NetView eq{a.params, 6, 1};
+  const NetView neq{a.params + net_size(6, 1, hidden, layers), 6 + L, 1};
+  const NetView evo{neq.base + net_size(6 + L, 1, hidden, layers), 6 + L, L};
+  for (int i = t; i < ER_TILE * 8; i += ER_THREADS) {
+    const int p = i >> 3, c = i & 7;
+    const bool live = p0 + p < a.n;
+    if (c < 6) eps[p * 6 + c] = live ? a.strain[(p0 + p) * 6 + c] / a.scale[c] : 0.0f;
+    zin[i] = (live && c < L) ? a.latent_in[(p0 + p) * L + c] : 0.0f;
+    if (c == 0) cdt[p] = live ? a.time_step[p0 + p] / a.tau : 0.0f;
+  }
+  __syncthreads();
+  auto set_input = [&](const float* latent) {  // s.x = [e^, latent]
+    for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
+      const int p = i / ER_XLD, c = i % ER_XLD;
+      s.x[sw(c, p)] = c < 6 ? eps[p * 6 + c] : (latent && c < 6 + L ? latent[p * 8 + c - 6] : 0.0f);
+    }
+    __syncthreads();
+  };
+  // s.x = (e_j, latent part per point (or 0))
+  auto set_direction = [&](int j, const float* latent_dir) {
+    for (int i = t; i < ER_TILE * ER_XLD; i += ER_THREADS) {
+      const int p = i / ER_XLD, c = i % ER_XLD;
+      s.x[sw(c, p)] = c < 6 ? (c == j ? 1.0f : 0.0f) : (latent_dir && c < 6 + L ? latent_dir[p * 48 + (c - 6) * 6 + j] : 0.0f);
+    }
+    __syncthreads();
+  };
+  // accumulate rows 0..5 of s.gin as column j of the tangent (thread p < TILE owns point p)
+  auto store_column = [&](int j, bool add) {
+    if (t < ER_TILE && p0 + t < a.n) {
+      float* out = a.tangent + (p0 + t) * 36;
+      for (int i = 0; i < 6; ++i) {
+        const float v = s.gin[sw(i, t)] / (a.scale[i] * a.scale[j]);
+        out[6 * i + j] = add ? out[6 * i + j] + v : v;
+      }
+    }
+    __syncthreads();
+  };
+  // 1. equilibrium potential: its Hessian in the strain block
+  set_input(nullptr);
+  tan_primal(eq, hidden, layers, s, true);
+  for (int j = 0; j < 6; ++j) {
+    set_direction(j, nullptr);
+    tan_forward(eq, hidden, layers, s);
+    tan_backward(eq, hidden, layers, s);
+    store_column(j, false);
+  }
+  // 2. non-equilibrium potential at the stress state, in the total strain direction
+  const float* latent_dir = nullptr;
+  const float* state = zin;
+  if (a.integrator == 1) {
+    set_input(zin);
+    const float* h = tan_primal(evo, hidden, layers, s, false);
+    const float* wo = output_ptr(evo, hidden, layers);
+    const float* bo = wo + (int64_t)L * hidden;
+    for (int i = t; i < ER_TILE * 8; i += ER_THREADS) {
+      const int p = i >> 3, o = i & 7;
+      float v = 0.0f;
+      if (o < L) {
+        v = bo[o];
+        for (int j = 0; j < hidden; ++j) v = fmaf(wo[(int64_t)o * hidden + j], h[sw(j, p)], v);
+      }
+      zc[i] = o < L ? zin[i] + cdt[p] * v : 0.0f;
+    }
+    __syncthreads();
+    for (int j = 0; j < 6; ++j) {
+      set_direction(j, nullptr);
+      const float* hd = tan_forward(evo, hidden, layers, s);
+      for (int i = t; i < ER_TILE * 8; i += ER_THREADS) {
+        const int p = i >> 3, o = i & 7;
+        float v = 0.0f;
+        if (o < L)
+          for (int k = 0; k < hidden; ++k) v = fmaf(wo[(int64_t)o * hidden + k], hd[sw(k, p)], v);
+        jf[p * 48 + o * 6 + j] = cdt[p] * v;
+      }
+      __syncthreads();
+    }
+    latent_dir = jf;
+    state = zc;
+  }
+  set_input(state);
+  tan_primal(neq, hidden, layers, s, true);
+  for (int j = 0; j < 6; ++j) {
+    set_direction(j, latent_dir);
+    tan_forward(neq, hidden, layers, s);
+    tan_backward(neq, hidden, layers, s);
+    store_column(j, true);
+  }
+}
+
+inline size_t tangent_smem(int hidden, int layers) {
+  const size_t floats = (size_t)ER_TILE * ER_XLD * 2 + (size_t)ER_TILE * hidden * (2 + 3 * layers - 1) +
+                        (size_t)ER_TILE * (6 + 8 + 8 + 48 + 1);
+  return floats * sizeof(float);
+}
+
 inline size_t energy_smem(int hidden, int layers) {
   const size_t floats = (size_t)ER_TILE * ER_XLD * 2 + (size_t)ER_TILE * hidden * (2 + layers) +
                         (size_t)ER_TILE * (6 + 8 + 8 + 8 + 6 + 16 + 16) + 3 * ER_TILE;
@@ -439,4 +718,24 @@ extern "C" int cib_energy_rno_update(const cib_energy_rno* model, int64_t n, con
   a.rate_dimless = dimensionless_rate;
   a.scalars = scalars;
   return launch_energy(model, a, (n + ER_TILE - 1) / ER_TILE, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int cib_energy_rno_tangent(const cib_energy_rno* model, int64_t n, const float* strain, const float* latent,
+                                      const float* time_step, float* tangent, void* stream) {
+  if (!valid_model(model) || n < 0 || !strain || !latent || !time_step || !tangent) return CIB_EINVAL;
+  if (model->layers < 2) return CIB_EINVAL;
+  if (n == 0) return CIB_OK;
+  const size_t smem = tangent_smem(model->hidden, model->layers);
+  if (smem > 227 * 1024) return CIB_ERANGE;  // e.g. more than 4 hidden layers of 128
+  const int rc = allow_dynamic_smem(reinterpret_cast<const void*>(energy_rno_tangent_kernel), 227 * 1024);
+  if (rc != CIB_OK) return rc;
+  EnergyArgs a = base_args(model);
+  a.n = n;
+  a.strain = strain;
+  a.latent_in = latent;
+  a.time_step = time_step;
+  a.tangent = tangent;
+  energy_rno_tangent_kernel<<<(unsigned)((n + ER_TILE - 1) / ER_TILE), ER_THREADS, smem,
+                              reinterpret_cast<cudaStream_t>(stream)>>>(a);
+  return check_launch();
 }

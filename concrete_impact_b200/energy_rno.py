@@ -9,9 +9,11 @@ FP32 kernel (csrc/energy_rno.cu) per call: per point, the equilibrium and non-eq
 potentials with their hand-written input gradients, the state-evolution network and the
 forward-Euler latent step.
 
-Scope: ``direct_rate`` evolution, FP32 models, no algorithmic tangent (``compute_tangent``
-raises; the reference computes it by automatic differentiation); training stays with the
-reference (the surrogate this package trains is ``rno.RNOSurrogate``).
+``compute_tangent`` adds the algorithmic tangent d stress / d strain, computed by a second
+kernel with forward-over-reverse second derivatives of the three networks (the reference
+differentiates the stress with autograd).  Scope: ``direct_rate`` evolution, FP32 models;
+training stays with the reference (the surrogate this package trains is
+``rno.RNOSurrogate``).
 """
 
 from __future__ import annotations
@@ -197,9 +199,9 @@ class EnergyDissipationRVERNO:
 
     def update_batch(self, strain, previous_latent, time_step, anchors: EnergyAnchors | None = None,
                      compute_tangent: bool = False) -> RVERNOUpdateBatch:  # fmt: skip
-        """Update all points at one time index (rve_rno.py:249-313, without the tangent)."""
-        if compute_tangent:
-            raise SurrogateCapabilityError("The GPU RVE-RNO does not provide the algorithmic tangent.")
+        """Update all points at one time index (rve_rno.py:249-313).  ``compute_tangent``
+        adds the algorithmic tangent d stress / d strain (n, 6, 6) from the second-derivative
+        kernel (cib_energy_rno_tangent), in place of the reference's autograd rows."""
         self._require_loaded()
         f32 = lambda a: (a if isinstance(a, torch.Tensor) else torch.as_tensor(np.asarray(a))).to(  # noqa: E731
             device=self.device, dtype=torch.float32).contiguous()
@@ -221,15 +223,23 @@ class EnergyDissipationRVERNO:
                                                      out["latent"].data_ptr(), out["rate"].data_ptr(),
                                                      out["dimless"].data_ptr(), out["scalars"].data_ptr(),
                                                      _native.stream_ptr()), "cib_energy_rno_update")  # fmt: skip
+        tangent = None
+        if compute_tangent:
+            tangent = torch.empty((n, 6, 6), dtype=torch.float32, device=self.device)
+            _native.check(self.lib.cib_energy_rno_tangent(ctypes.byref(m), n, eps.data_ptr(), z.data_ptr(),
+                                                          dt.data_ptr(), tangent.data_ptr(), _native.stream_ptr()),
+                          "cib_energy_rno_tangent")  # fmt: skip
         s = out["scalars"]
-        return RVERNOUpdateBatch(out["stress"], out["latent"], out["rate"], out["dimless"], s[0], s[1], s[2], s[3])
+        return RVERNOUpdateBatch(out["stress"], out["latent"], out["rate"], out["dimless"], s[0], s[1], s[2], s[3],
+                                 tangent)
 
     def update(self, strain, previous_latent, time_step, compute_tangent: bool = False, context=None):
         """Batch of one (rve_rno.py:420-453)."""
         res = self.update_batch(torch.as_tensor(np.asarray(strain, dtype=np.float32)).reshape(1, 6),
                                 torch.as_tensor(np.asarray(previous_latent, dtype=np.float32)).reshape(1, -1),
                                 torch.as_tensor([float(time_step)], dtype=torch.float32), None, compute_tangent)  # fmt: skip
-        return RVERNOUpdateBatch(*(getattr(res, f)[0] if f != "tangent" else None for f in RVERNOUpdateBatch.__dataclass_fields__))
+        return RVERNOUpdateBatch(*(getattr(res, f)[0] if getattr(res, f) is not None else None
+                                   for f in RVERNOUpdateBatch.__dataclass_fields__))
 
     def _require_loaded(self) -> None:
         if not self.loaded:
@@ -282,17 +292,19 @@ class RVERNOMaterialAdapter:
         latent = state.variables["latent_state"]
         if request.strains.shape[0] != latent.shape[0]:
             raise ValueError("RVE-RNO strain and latent-state point counts differ.")
-        if requirements.tangent:
-            raise SurrogateCapabilityError("RVE-RNO tangent was requested but not returned.")
         host = not isinstance(request.strains, torch.Tensor)
         if self._anchors is None:
             self._anchors = self.model.prepare_energy_anchors()
         n = int(request.strains.shape[0])
         res = self.model.update_batch(request.strains, latent,
-                                      torch.full((n,), float(request.time_step), dtype=torch.float32), self._anchors)  # fmt: skip
+                                      torch.full((n,), float(request.time_step), dtype=torch.float32), self._anchors,
+                                      compute_tangent=requirements.tangent)  # fmt: skip
+        if requirements.tangent and res.tangent is None:
+            raise SurrogateCapabilityError("RVE-RNO tangent was requested but not returned.")
         out = (lambda t: t.double().cpu().numpy()) if host else (lambda t: t.double())  # noqa: E731
         return MaterialPointResponse(
-            stresses=out(res.stress), state=MaterialState({"latent_state": out(res.latent_state)}), tangents=None,
+            stresses=out(res.stress), state=MaterialState({"latent_state": out(res.latent_state)}),
+            tangents=out(res.tangent) if requirements.tangent else None,
             dissipation=out(res.dissipation) if requirements.dissipation else None,
             free_energy=out(res.free_energy) if requirements.free_energy else None,
             diagnostics={"thermodynamic_violation": out(res.thermodynamic_violation),

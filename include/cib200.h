@@ -606,6 +606,15 @@ int cib_energy_rno_update(const cib_energy_rno* model, int64_t n, const float* s
                           const float* time_step, const float* anchors, float* stress, float* latent_out,
                           float* state_rate, float* dimensionless_rate, float* scalars, void* stream);
 
+/* Algorithmic tangent d stress / d strain of the update above, (n, 6, 6) FP32 row-major
+ * [i][j] = d stress_i / d strain_j -- the rows the reference obtains by autograd
+ * (rve_rno.py:283-297): second derivatives of the two potentials by forward-over-reverse
+ * passes through the networks, through the candidate latent state (strain Jacobian of the
+ * evolution network) for the current-state integrator.  2 to 4 hidden layers of up to 128
+ * (CIB_ERANGE beyond what fits in shared memory). */
+int cib_energy_rno_tangent(const cib_energy_rno* model, int64_t n, const float* strain, const float* latent,
+                           const float* time_step, float* tangent, void* stream);
+
 /* Error gate of the surrogate at n macro points (no reference counterpart; the reference's
  * deployment adapter, src/concrete_impact/nn/deployment.py:68-165, has no input gate).
  * prepare: strain_n = strain / strain_scale, rate_n = rate / rate_scale (fp32, n x 6),
