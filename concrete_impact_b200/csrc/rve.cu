@@ -304,8 +304,10 @@ __device__ __forceinline__ void load_w(const double* w, const double* dw, double
 // forces and Jacobi diagonal contributions.  The grid covers all Gauss points of the batch
 // (one thread each, grid-stride in whole waves), whatever RVE they belong to, so an uneven
 // batch keeps every SM busy until the last element; each 8-lane group looks up its RVE.
+// FP32: capped at 80 registers for three CTAs (24 warps) per SM, 32 B of spills; FP64 keeps
+// its 170 registers.
 template <typename T>
-__global__ void __launch_bounds__(RVE_THREADS) rve_residual_kernel(const RveResidualArgs<T> a) {
+__global__ void __launch_bounds__(RVE_THREADS, sizeof(T) == 4 ? 3 : 1) rve_residual_kernel(const RveResidualArgs<T> a) {
   const int64_t G_all = 8 * a.nelem;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t rounds = (G_all + stride - 1) / stride;  // the same for every thread (shuffles)
@@ -531,6 +533,79 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_gather_norms_kernel(const Rve
 }
 
 // ---------------------------------------------------------------------------------------
+// One element-Gauss-point item of the matrix-free apply and its loads.  The apply loops
+// fetch the next round's item (the vector values at its node, its phase and tangent flag,
+// then its tangent parameters) while the current round computes, so that the L2 latency of
+// those loads overlaps the arithmetic instead of stalling every round.
+template <typename T>
+struct ApplyItem {
+  bool live;
+  int el, q, ph, flag;
+  int64_t g;
+  T mine[3];
+  T tp[8];
+};
+
+template <typename T>
+__device__ __forceinline__ void fetch_item(const RvePcgArgs<T>& a, const RveDesc& d, const double* __restrict__ p,
+                                           int items, int nxy, int k, int it, ApplyItem<T>& x) {
+  const int gl = it * blockDim.x + threadIdx.x;
+  x.live = gl < items;
+  x.el = x.live ? (gl >> 3) : 0;
+  x.q = gl & 7;
+  const int j = x.el / d.nx, i = x.el - j * d.nx;
+  const int64_t e = d.eoff + x.el + (int64_t)nxy * k;
+  x.g = 8 * e + x.q;
+  x.ph = 0;
+  x.flag = 0;
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) x.mine[dd] = (T)0;
+  if (x.live) {
+    const int64_t node = element_node(d, i, j, k, x.q);
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) x.mine[dd] = (T)__ldcg(p + 3 * node + dd);  // other ranks may have written p
+    x.ph = (int)a.phase[e];
+    x.flag = (int)a.tflag[x.g];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void fetch_tangent(const RvePcgArgs<T>& a, ApplyItem<T>& x) {
+  if (x.live && x.flag) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) x.tp[c] = a.tparam[c * a.ngp + x.g];
+  }
+}
+
+// Element-node contributions w B^T C B u of one item (valid on every lane; zero when the
+// item is not live), reduce-scattered so that lane q holds node q's three values.
+template <typename T>
+__device__ __forceinline__ void apply_item(const RvePcgArgs<T>& a, const ApplyItem<T>& x, const T* gtab, T jw,
+                                           T out[3]) {
+  T u[8][3];
+  allgather8(x.mine, u);
+  Grad8<T> Gr;
+  load_grads(gtab, x.q, Gr);
+  T eps[6], sig[6];
+  strain_from(Gr, u, eps);
+  TangentParams<T> tp;
+  tp.elastic = 1;
+  tp.f = (T)0;
+  tp.c = (T)0;
+  if (x.live && x.flag) {
+    tp.elastic = 0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tp.n[c] = x.tp[c];
+    tp.f = x.tp[6];
+    tp.c = x.tp[7];
+  }
+  tangent_apply(a.mats.m[x.ph], tp, eps, sig);
+  T f[8][3];
+  bt_stress(Gr, sig, x.live ? jw : (T)0, f);
+  reduce_scatter8(f, x.q, out);
+}
+
+// ---------------------------------------------------------------------------------------
 // Matrix-free apply of the reduced tangent to one periodic vector, streaming the RVE in
 // z-layers: element results of a layer go to shared memory, then every node of the layer
 // gathers its 4 bottom and 4 top contributions in a fixed order.  Returns p . Ap (CTA-wide).
@@ -547,46 +622,20 @@ __device__ double apply_tangent(const RvePcgArgs<T>& a, const RveDesc& d, const 
   const int items = 8 * nxy;
   const int rounds = (items + blockDim.x - 1) / blockDim.x;
   for (int k = 0; k < d.nz; ++k) {
+    ApplyItem<T> cur, nxt;
+    fetch_item(a, d, p, items, nxy, k, 0, cur);
+    fetch_tangent(a, cur);
     for (int it = 0; it < rounds; ++it) {
-      const int gl = it * blockDim.x + threadIdx.x;
-      const bool live = gl < items;
-      const int el = live ? (gl >> 3) : 0;
-      const int q = gl & 7;
-      const int j = el / d.nx, i = el - j * d.nx;
-      const int64_t e = d.eoff + el + (int64_t)nxy * k;
-      T mine[3] = {0, 0, 0};
-      if (live) {
-        const int64_t node = element_node(d, i, j, k, q);
-#pragma unroll
-        for (int dd = 0; dd < 3; ++dd) mine[dd] = (T)p[3 * node + dd];
-      }
-      T u[8][3];
-      allgather8(mine, u);
-      Grad8<T> Gr;
-      load_grads(gtab, q, Gr);
-      T eps[6], sig[6];
-      strain_from(Gr, u, eps);
-      const int64_t g = 8 * e + q;
-      const int ph = live ? (int)a.phase[e] : 0;
-      TangentParams<T> tp;
-      tp.elastic = 1;
-      tp.f = (T)0;
-      tp.c = (T)0;
-      if (live && a.tflag[g]) {
-        tp.elastic = 0;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) tp.n[c] = a.tparam[c * a.ngp + g];
-        tp.f = a.tparam[6 * a.ngp + g];
-        tp.c = a.tparam[7 * a.ngp + g];
-      }
-      tangent_apply(a.mats.m[ph], tp, eps, sig);
-      T f[8][3];
-      bt_stress(Gr, sig, live ? jw : (T)0, f);
+      if (it + 1 < rounds) fetch_item(a, d, p, items, nxy, k, it + 1, nxt);
       T out[3];
-      reduce_scatter8(f, q, out);
-      if (live)
+      apply_item(a, cur, gtab, jw, out);
+      if (cur.live)
 #pragma unroll
-        for (int dd = 0; dd < 3; ++dd) ye[(8 * el + q) * 3 + dd] = (double)out[dd];
+        for (int dd = 0; dd < 3; ++dd) ye[(8 * cur.el + cur.q) * 3 + dd] = (double)out[dd];
+      if (it + 1 < rounds) {
+        fetch_tangent(a, nxt);
+        cur = nxt;
+      }
     }
     __syncthreads();
     for (int n = threadIdx.x; n < nxy; n += blockDim.x) {
@@ -767,46 +816,20 @@ __device__ double apply_tangent_slab(const RvePcgArgs<T>& a, const RveDesc& d, c
   const int items = 8 * nxy;
   const int rounds = (items + blockDim.x - 1) / blockDim.x;
   for (int k = k0; k < k1; ++k) {
+    ApplyItem<T> cur, nxt;
+    fetch_item(a, d, p, items, nxy, k, 0, cur);
+    fetch_tangent(a, cur);
     for (int it = 0; it < rounds; ++it) {
-      const int gl = it * blockDim.x + threadIdx.x;
-      const bool live = gl < items;
-      const int el = live ? (gl >> 3) : 0;
-      const int q = gl & 7;
-      const int j = el / d.nx, i = el - j * d.nx;
-      const int64_t e = d.eoff + el + (int64_t)nxy * k;
-      T mine[3] = {0, 0, 0};
-      if (live) {
-        const int64_t node = element_node(d, i, j, k, q);
-#pragma unroll
-        for (int dd = 0; dd < 3; ++dd) mine[dd] = (T)__ldcg(p + 3 * node + dd);  // other ranks wrote p
-      }
-      T u[8][3];
-      allgather8(mine, u);
-      Grad8<T> Gr;
-      load_grads(gtab, q, Gr);
-      T eps[6], sig[6];
-      strain_from(Gr, u, eps);
-      const int64_t g = 8 * e + q;
-      const int ph = live ? (int)a.phase[e] : 0;
-      TangentParams<T> tp;
-      tp.elastic = 1;
-      tp.f = (T)0;
-      tp.c = (T)0;
-      if (live && a.tflag[g]) {
-        tp.elastic = 0;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) tp.n[c] = a.tparam[c * a.ngp + g];
-        tp.f = a.tparam[6 * a.ngp + g];
-        tp.c = a.tparam[7 * a.ngp + g];
-      }
-      tangent_apply(a.mats.m[ph], tp, eps, sig);
-      T f[8][3];
-      bt_stress(Gr, sig, live ? jw : (T)0, f);
+      if (it + 1 < rounds) fetch_item(a, d, p, items, nxy, k, it + 1, nxt);
       T out[3];
-      reduce_scatter8(f, q, out);
-      if (live)
+      apply_item(a, cur, gtab, jw, out);
+      if (cur.live)
 #pragma unroll
-        for (int dd = 0; dd < 3; ++dd) ye[(8 * el + q) * 3 + dd] = out[dd];
+        for (int dd = 0; dd < 3; ++dd) ye[(8 * cur.el + cur.q) * 3 + dd] = out[dd];
+      if (it + 1 < rounds) {
+        fetch_tangent(a, nxt);
+        cur = nxt;
+      }
     }
     __syncthreads();
     for (int n = threadIdx.x; n < nxy; n += blockDim.x) {

@@ -2,8 +2,9 @@
  * cib200.h -- C ABI of the B200 (sm_100a) material-point and periodic-RVE kernels.
  *
  * Every entry point takes plain device pointers, sizes and a CUDA stream (passed as
- * `void*`, NULL = legacy default stream).  Nothing here allocates device memory: all
- * buffers, including solver work vectors, are passed in by the caller.  All calls are
+ * `void*`, NULL = legacy default stream).  Nothing here allocates device memory for data:
+ * all buffers, including solver work vectors, are passed in by the caller (the one
+ * exception is cib_rve_newton_graph_create, which builds and instantiates a CUDA graph).  All calls are
  * asynchronous on the given stream.  The integer return value reports argument and
  * launch errors only (0 = launched); per-point numerical failures are reported through
  * the `first_failure` word, which the caller initialises to CIB_NO_FAILURE and reads
