@@ -91,7 +91,7 @@ def _rve_path_cpu(gpu_out: dict, sample_steps: int = 3) -> dict:
     return {"value": gpu_out["steps"] / est, "unit": "RVE steps/s", "cores": 1, "kind": "port",
             "sample": f"oracle (NumPy/SciPy direct solves) on the first {sample_steps} path steps at the GPU run's "
                       f"converged macro strains, {per_solve:.3f} s per solve x {gpu_out['solves']} solves",
-            "max_rel_stress_diff_vs_gpu": max(diffs)}  # fmt: skip
+            "max_rel_stress_diff_vs_oracle": max(diffs)}  # fmt: skip
 
 
 def run_rve_path(args: argparse.Namespace) -> None:
@@ -110,6 +110,14 @@ def run_rve_path(args: argparse.Namespace) -> None:
     if rank != 0:
         return
     cpu = None if args.no_cpu_baseline else _rve_path_cpu(out)
+    ref, meta = _golden("rve_path_uniaxial_8")
+    parity = {"max_rel_stress_diff_vs_reference": None}
+    if ref is not None and len(out["macro_stress"]) >= meta["steps"]:
+        got = np.asarray(out["macro_stress"][: meta["steps"]])
+        scale = np.abs(ref["macro_stress"]).max(axis=1)
+        parity = {"max_rel_stress_diff_vs_reference": float((np.abs(got - ref["macro_stress"]).max(axis=1) / scale).max()),
+                  "sample": f"first {meta['steps']} steps against the reference's solve_rve_microequilibrium in the "
+                            "same mixed-control loop"}  # fmt: skip
     seconds = out["ms"] / 1e3
     value = out["steps"] / seconds
     # one 8^3 RVE occupies at most one cluster of CTAs: a latency-bound solve, not a
@@ -117,7 +125,7 @@ def run_rve_path(args: argparse.Namespace) -> None:
     peak, kind = _peak()
     line = _line(args, "accepted RVE steps/s (8^3 concrete RVE, mixed-control uniaxial path, FP64)", value,
                  "RVE steps/s", "rve_path: 8^3 two-phase RVE, seed 0, uniaxial compression -0.5 % in 100 steps at 10/s",
-                 {"ms_per_step": out["ms"] / out["steps"], "dtype": "f64", "pcg_cluster": cluster,
+                 {"ms_per_step": out["ms"] / out["steps"], "dtype": "f64", "pcg_cluster": cluster, "parity": parity,
                   "gp_evaluations_per_s": out["gp_evaluations"] / seconds,
                   "solves": out["solves"], "newton_iterations": out["newton_iterations"],
                   "pcg_iterations": out["pcg_iterations"],
@@ -174,6 +182,50 @@ def _rve_batch_cpu(setup, sample_edges=(8, 12)) -> dict:
             "sample_seconds": seconds}  # fmt: skip
 
 
+def _golden(name: str):
+    """Arrays and metadata of a committed golden run of the reference (tests/golden)."""
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent / "tests" / "golden"
+    manifest = json.loads((root / "manifest.json").read_text())
+    if name not in manifest or not (root / f"{name}.npz").exists():
+        return None, None
+    with np.load(root / f"{name}.npz") as data:
+        return {k: data[k] for k in data.files}, manifest[name]
+
+
+def _rve_batch_reference_parity(precision: int = 32, forcing: str | None = "eisenstat_walker") -> dict:
+    """The workload's RVEs of every edge (the reference's own solves, tests/golden
+    rve_batch_edge*) re-solved as one uneven batch with the workload's settings: the largest
+    relative homogenised-stress difference over members and steps."""
+    import torch
+
+    from concrete_impact_b200.benchmarks import UPDATE_SETTINGS, concrete_rve
+    from concrete_impact_b200.rve import RS_SIGMA, LinearSolverOptions, RVEBatch, solve_batch_step
+
+    cases = [_golden(f"rve_batch_edge{e}") for e in EDGES]
+    if any(a is None for a, _ in cases):
+        return {"max_rel_stress_diff_vs_reference": None, "note": "reference golden runs not present"}
+    models = [concrete_rve(m["edge"], m["layout_seed"], precision) for _, m in cases]
+    batch = RVEBatch(models, precision=precision, linear_solver=LinearSolverOptions(cluster="auto", forcing=forcing),
+                     device_control=True)  # fmt: skip
+    vol = torch.as_tensor(batch.volumes, device=batch.device)[:, None]
+    worst = 0.0
+    for step in range(cases[0][0]["macro_strain"].shape[0]):
+        batch.macro.copy_(torch.as_tensor(np.stack([a["macro_strain"][step] for a, _ in cases]), device=batch.device))
+        batch.dt.copy_(torch.as_tensor([a["time_step"][step] for a, _ in cases], device=batch.device))
+        solve_batch_step(batch, models[0].newton_settings, UPDATE_SETTINGS, False)
+        batch.response(batch.batch_struct(UPDATE_SETTINGS), batch.w, None, None)
+        got = (batch.sums[:, RS_SIGMA : RS_SIGMA + 6] / vol).cpu().numpy()
+        batch.commit()
+        for r, (a, _) in enumerate(cases):
+            ref = a["macro_stress"][step]
+            worst = max(worst, float(np.abs(got[r] - ref).max() / np.abs(ref).max()))
+    return {"max_rel_stress_diff_vs_reference": worst,
+            "sample": "one RVE of each edge 8..24 of this workload (its layout and path), time indices 0, 10, 20, 30, "
+                      "against the reference's solve_rve_microequilibrium (FP64 direct solves)"}  # fmt: skip
+
+
 def run_rve_batch(args: argparse.Namespace) -> None:
     import torch
 
@@ -209,6 +261,7 @@ def run_rve_batch(args: argparse.Namespace) -> None:
                          f"steps, {c['per_element_step_s'] * 1e6:.1f} us per element-step scaled to "
                          f"{c['total_elements']:,} elements"}  # fmt: skip
     rve_steps_s = out["rve_steps"] / seconds
+    parity = _rve_batch_reference_parity()
     line = _line(args, "micro Gauss-point evaluations/s inside the batched RVE Newton solve (256 uneven RVEs)", value,
                  "GP/s", "rve_batch: 256 two-phase RVEs, edges {8,12,16,20,24}, random 4-segment paths, FP32 elements",
                  {"ms_per_step": out["ms"] / args.steps, "dtype": "f32 elements, f64 reductions and history",
@@ -219,7 +272,7 @@ def run_rve_batch(args: argparse.Namespace) -> None:
                   "pcg_tuning": {"ms": (out["tuning"] or {}).get("ms"), "cached": (out["tuning"] or {}).get("cached"),
                                  "key": "cluster size / launch shape (0: 256 threads default cap, 1: 128 threads, "
                                         "2: 512 threads, 3: 256 threads other register cap)"},
-                  "newton_forcing": out["forcing"],
+                  "newton_forcing": out["forcing"], "parity": parity,
                   "newton_control": ("device: one CUDA graph per step (conditional while loop over the Newton "
                                      "iterations; residual, gather x2, check, PCG, update, axpy kernels per iteration)"
                                      if out["device_control"] else "host loop (two read-backs per Newton iteration)"),
@@ -460,7 +513,7 @@ def _rve_ogrid_cpu(gpu_out: dict | None = None, sample_steps: int = 2) -> dict:
     line = {"value": 1.0 / per_step, "unit": "RVE steps/s", "cores": 1, "kind": "port",
             "sample": f"general-mesh RVE oracle on the first {sample_steps} path steps, {per_step:.3f} s per step"}  # fmt: skip
     if diffs:
-        line["max_rel_stress_diff_vs_gpu"] = max(diffs)
+        line["max_rel_stress_diff_vs_oracle"] = max(diffs)
     return line
 
 

@@ -15,6 +15,7 @@ the kernels of ``csrc/hex8.cu`` with a deterministic (fixed-order, atomic-free) 
 
 from __future__ import annotations
 
+import warnings
 from dataclasses import dataclass, field
 from typing import Any
 
@@ -209,9 +210,13 @@ def assemble_hex8_material_response_cached(nodes, elements, material, committed_
         if io.host:
             tangent = csr_matrix((values.cpu().numpy(), cache.csr_indices, cache.csr_indptr), shape=(n_dof, n_dof))
         else:
-            tangent = torch.sparse_csr_tensor(torch.as_tensor(cache.csr_indptr, device=dev),
-                                              torch.as_tensor(cache.csr_indices, device=dev), values,
-                                              size=(n_dof, n_dof), check_invariants=False)  # fmt: skip
+            # the pattern is the cache's own sorted CSR pattern: skip torch's invariant check
+            # (and its notices that CSR support is beta and the check is off)
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore", UserWarning)
+                tangent = torch.sparse_csr_tensor(torch.as_tensor(cache.csr_indptr, device=dev),
+                                                  torch.as_tensor(cache.csr_indices, device=dev), values,
+                                                  size=(n_dof, n_dof), check_invariants=False)  # fmt: skip
     else:
         tangent = csr_matrix((n_dof, n_dof)) if io.host else None
     return NonlinearSolidAssemblyResult(
