@@ -292,15 +292,17 @@ class FE2Recipe:
     """How the deployed surrogate is trained: random 6-component RVE paths (general states;
     they also keep the surrogate stable when a macro solver drives it) plus impact paths taken
     from direct FE^2 runs of a calibration bar at other pulse amplitudes (the reference's
-    impact_path data source)."""
+    impact_path data source).  The calibration bar has a confined core (64 x 8 x 8): a
+    surrogate calibrated on a 64 x 2 x 2 bar, all free surface, reached 2.2 % open-loop
+    error on that bar but 10.7 % on the 64 x 16 x 16 bar."""
 
     random_paths: int = 1000
     random_amplitude: tuple[float, float] = (2.0e-4, 5.0e-3)
     path_steps: int = 400
     impact_amplitudes: tuple[float, ...] = (20.0e6, 30.0e6, 40.0e6, 60.0e6, 70.0e6, 80.0e6)
-    calibration_divisions: tuple[int, int, int] = (64, 2, 2)
-    point_stride: int = 2
-    epochs: int = 2500
+    calibration_divisions: tuple[int, int, int] = (64, 8, 8)
+    point_stride: int = 16
+    epochs: int = 1500
     tau_ref: float = 1.0e-4
     learning_rate: float = 1.0e-3
     final_lr_fraction: float = 0.02
@@ -446,7 +448,7 @@ def fe2_closed_loop(rno, envelope, steps: int = 400, divisions=(64, 16, 16), fal
 
 
 def fe2_judged(rno, envelope, steps: int = 5000, warmup: int = 5, divisions=(64, 16, 16), sample: int = 256,
-               every: int = 1, threshold: float = 0.05, fallback_capacity: int = 32768, seed: int = 0) -> dict:  # fmt: skip
+               every: int = 1, threshold: float | None = 0.05, fallback_capacity: int = 32768, seed: int = 0) -> dict:  # fmt: skip
     """Surrogate FE^2 on the full bar with the runtime judge (``SurrogateJudge``: FP64
     direct RVEs at ``sample`` seeded macro points, every ``every`` steps): macro steps/s
     with the judge's cost included, the judged homogenised-stress error over the run and

@@ -165,21 +165,23 @@ class SurrogateJudge:
     compared with the direct homogenised stress; the judge keeps the squared errors and
     squared reference stresses per point, so ``error`` is the relative Frobenius error of
     the homogenised stress over the sampled points and judge steps.  A sampled point whose
-    own relative error exceeds ``threshold`` (once its reference stress exceeds
-    ``stress_floor``) is escalated: it leaves the surrogate for the fallback pool, which
-    takes over the judge's RVE state of that point (its exact history).  One host read per
-    judge step decides the escalations.
+    own error exceeds ``threshold`` relative to its reference stress, or to
+    ``stress_floor`` where that is larger (so that the arrival of a wave front, when the
+    stress is still near zero, is not judged relative to nothing), is escalated: it leaves
+    the surrogate for the fallback pool, which takes over the judge's RVE state of that
+    point (its exact history).  ``threshold`` None only measures.  One host read per judge
+    step decides the escalations.
     """
 
     def __init__(self, model: StructuredHex8RVE, n_points: int, update_settings: MaterialUpdateSettings,
-                 sample: int = 256, every: int = 1, threshold: float = 0.05, stress_floor: float = 1.0e6,
+                 sample: int = 256, every: int = 1, threshold: float | None = 0.05, stress_floor: float = 1.0e6,
                  seed: int = 0, precision: int = 64) -> None:  # fmt: skip
         rng = np.random.default_rng(seed)
         pts = np.sort(rng.choice(n_points, size=min(sample, n_points), replace=False))
         self.model = model
         self.settings = update_settings
         self.every = max(int(every), 1)
-        self.threshold = float(threshold)
+        self.threshold = None if threshold is None else float(threshold)
         self.floor2 = float(stress_floor) ** 2
         self.batch = RVEBatch([model] * pts.size, precision=precision, device_control=True)
         dev = self.batch.device
@@ -187,6 +189,7 @@ class SurrogateJudge:
         self.volume = float(self.batch.volumes[0])
         self.sq_err = torch.zeros(pts.size, dtype=torch.float64, device=dev)
         self.sq_ref = torch.zeros(pts.size, dtype=torch.float64, device=dev)
+        self.sq_den = torch.zeros(pts.size, dtype=torch.float64, device=dev)  # sum of max(|ref|^2, floor^2)
         self.escalated = torch.zeros(pts.size, dtype=torch.bool, device=dev)
         self.count = 0
         self.elapsed = 0.0
@@ -215,13 +218,17 @@ class SurrogateJudge:
         b.commit()
         self.reference = ref
         diff = delivered[self.points] - ref
+        ref2 = (ref * ref).sum(dim=1)
         self.sq_err += (diff * diff).sum(dim=1)
-        self.sq_ref += (ref * ref).sum(dim=1)
+        self.sq_ref += ref2
+        self.sq_den += ref2.clamp(min=self.floor2)
         self.judge_steps += 1
-        point_err2 = self.sq_err / self.sq_ref.clamp(min=1e-300)
-        bad = (point_err2 > self.threshold**2) & (self.sq_ref > self.floor2 * self.judge_steps) & ~self.escalated
+        point_err2 = self.sq_err / self.sq_den
         worst = float(point_err2.max().sqrt())
         self.history.append((self.count, self.error, worst))
+        if self.threshold is None:
+            return None
+        bad = (point_err2 > self.threshold**2) & ~self.escalated
         slots = torch.nonzero(bad).flatten()
         if slots.numel() == 0:
             return None

@@ -456,11 +456,14 @@ class RVEBatch:
         self._graphs: dict = {}
 
     # -- C structs ---------------------------------------------------------------------
-    def batch_struct(self, settings: MaterialUpdateSettings) -> _native.RVEBatchC:
+    def batch_struct(self, settings: MaterialUpdateSettings, prefix: int | None = None) -> _native.RVEBatchC:
+        """The C view of the batch; ``prefix`` restricts it to RVEs [0, prefix) (the kernels
+        that cover every element or node of a batch then launch over that range only)."""
         b = _native.RVEBatchC()
-        b.nrve = self.nrve
+        m = self.nrve if prefix is None else int(prefix)
+        b.nrve = m
         b.nphase = len(self.phases)
-        b.nelem = self.nelem
+        b.nelem = self.nelem if m == self.nrve else int(self.elem_offsets[m]) if m < self.nrve else self.nelem
         b.precision = self.precision
         b.max_nxy = self.max_nxy
         b.desc = self.desc.data_ptr()
@@ -557,14 +560,17 @@ class RVEBatch:
         )  # fmt: skip
         _native.check(code, "cib_rve_response")
 
-    def newton_graph(self, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings) -> "_NewtonGraph":
+    def newton_graph(self, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings,
+                     prefix: int | None = None) -> "_NewtonGraph":  # fmt: skip
         """The device-controlled Newton graph for these settings (built once, then reused;
-        the PCG cluster size and tolerances in force are part of the key)."""
+        the PCG cluster size and tolerances in force and the RVE prefix it covers are part
+        of the key)."""
+        prefix = self.nrve if prefix is None else int(prefix)
         key = (tuple(_newton_key(newton)), repr(update_settings), self.pcg_launch(), float(self.rtol),
-               int(self.linear.max_iterations), self.linear.forcing)  # fmt: skip
+               int(self.linear.max_iterations), self.linear.forcing, prefix)  # fmt: skip
         graph = self._graphs.get(key)
         if graph is None:
-            graph = _NewtonGraph(self, newton, update_settings)
+            graph = _NewtonGraph(self, newton, update_settings, prefix)
             self._graphs[key] = graph
         return graph
 
@@ -592,6 +598,18 @@ class RVEBatch:
         self.macro_n.copy_(self.macro)
 
 
+def _live_prefix(batch: RVEBatch, live_mask) -> int:
+    """Smallest power of two (capped at the batch size) covering every live RVE: a fallback
+    pool whose first slots are in use launches over those slots only."""
+    if live_mask is None:
+        return batch.nrve
+    live = np.flatnonzero(np.asarray(live_mask, dtype=bool))
+    if live.size == 0:
+        return min(1, batch.nrve)
+    need = int(live[-1]) + 1
+    return min(batch.nrve, 1 << (need - 1).bit_length())
+
+
 # --------------------------------------------------------------------------------------
 # Device-controlled Newton solve: one CUDA graph per step (csrc/rve_newton.cu).
 
@@ -607,15 +625,17 @@ def _newton_key(newton: NonlinearNewtonSettings) -> list:
 class _NewtonGraph:
     """Workspaces and the instantiated graph of ``cib_rve_newton_graph_create``."""
 
-    def __init__(self, batch: RVEBatch, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings) -> None:
+    def __init__(self, batch: RVEBatch, newton: NonlinearNewtonSettings, update_settings: MaterialUpdateSettings,
+                 prefix: int) -> None:  # fmt: skip
         lib = batch.lib
+        self.prefix = prefix
         n_int, n_double = ctypes.c_int64(), ctypes.c_int64()
-        lib.cib_rve_newton_workspace(batch.nrve, ctypes.byref(n_int), ctypes.byref(n_double))
+        lib.cib_rve_newton_workspace(prefix, ctypes.byref(n_int), ctypes.byref(n_double))
         dev = batch.device
         self.iwork = torch.zeros(n_int.value, dtype=torch.int32, device=dev)
         self.dwork = torch.zeros(n_double.value, dtype=torch.float64, device=dev)
         self.batch = batch
-        self.b = batch.batch_struct(update_settings)
+        self.b = batch.batch_struct(update_settings, prefix)
         s = _native.RVENewtonC()
         s.max_iterations = int(newton.max_iterations)
         s.inexact = 1 if batch.linear.forcing == "eisenstat_walker" else 0
@@ -658,13 +678,17 @@ def _solve_batch_step_graph(batch: RVEBatch, newton: NonlinearNewtonSettings, up
                             failure_context, live_mask) -> BatchStepResult:  # fmt: skip
     """solve_batch_step on the device: one graph launch, one read-back of the records."""
     R = batch.nrve
-    graph = batch.newton_graph(newton, update_settings)
+    prefix = _live_prefix(batch, live_mask)
+    graph = batch.newton_graph(newton, update_settings, prefix)
     if live_mask is None:
         batch.live_mask.fill_(1)
     else:
         batch.live_mask.copy_(torch.as_tensor(np.asarray(live_mask, dtype=np.int32), device=batch.device))
     graph.launch()
+    if prefix < R:  # RVEs beyond the prefix take no part: inactive, as in the host loop
+        batch.active[prefix:] = 0
     iw = graph.iwork.cpu().numpy()
+    R = prefix
     batch.last_graph_iterations = int(iw[0])  # loop bodies run (for launch accounting)
     dw = graph.dwork.cpu().numpy()
     its, pcg = iw[_CTL : _CTL + R].astype(np.int64), iw[_CTL + R : _CTL + 2 * R].astype(np.int64)
@@ -683,8 +707,16 @@ def _solve_batch_step_graph(batch: RVEBatch, newton: NonlinearNewtonSettings, up
         d = _failure_diag(batch, r, int(iw[0]) - 1, rnorm[r], tol[r], float(inc[r]), inc_tol[r])
         d["linear_solver_status"] = info
         raise RVEEquilibriumError("non_finite_increment", d)
-    live = np.ones(R, dtype=bool) if live_mask is None else np.asarray(live_mask, dtype=bool)
-    return BatchStepResult(its, np.zeros(R, dtype=np.int64), np.where(live, rnorm, 0.0), np.where(live, tol, 0.0), pcg)
+    full = batch.nrve
+    live = np.ones(full, dtype=bool) if live_mask is None else np.asarray(live_mask, dtype=bool)
+
+    def padded(v, dtype=None):  # per-RVE records of the whole batch (zeros beyond the prefix)
+        out = np.zeros(full, dtype=dtype or v.dtype)
+        out[:R] = v
+        return out
+
+    return BatchStepResult(padded(its), np.zeros(full, dtype=np.int64), np.where(live, padded(rnorm), 0.0),
+                           np.where(live, padded(tol), 0.0), padded(pcg))  # fmt: skip
 
 
 # --------------------------------------------------------------------------------------
@@ -727,7 +759,8 @@ def solve_batch_step(
     if batch.device_control and not newton.armijo.enabled and timers is None:
         return _solve_batch_step_graph(batch, newton, update_settings, failure_context, live_mask)
     R = batch.nrve
-    b = batch.batch_struct(update_settings)
+    prefix = _live_prefix(batch, live_mask)
+    b = batch.batch_struct(update_settings, prefix)
     batch.w.copy_(batch.w_n)
     done = np.zeros(R, dtype=bool) if live_mask is None else ~np.asarray(live_mask, dtype=bool)
     final_active = None if live_mask is None else np.asarray(live_mask, dtype=bool).copy()
@@ -778,7 +811,7 @@ def solve_batch_step(
                 eta = min(new_eta, 0.1)
             rtol = max(float(batch.rtol), eta)
         prev_rnorm = np.where(live, rnorm, prev_rnorm)
-        _timed(timers, "pcg", lambda: batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, R, batch.sys_rve,
+        _timed(timers, "pcg", lambda: batch.pcg(b, batch.res, batch.x, batch.r, batch.p, batch.Ap, prefix, batch.sys_rve,
                                                 batch.sys_off, batch.pcg_status, batch.pcg_iters, batch.pcg_rel,
                                                 batch.pcg_xnorm, rtol))  # fmt: skip
         status, piters, xnorm = (t.cpu().numpy() for t in (batch.pcg_status, batch.pcg_iters, batch.pcg_xnorm))

@@ -237,13 +237,13 @@ def test_judge_measures_the_delivered_stress_against_direct_rves() -> None:
     dt = stable_time_step(bar, MORTAR.maximum_wave_speed, 0.5)
     rve = build_structured_rve((2, 2, 2), MORTAR, default_newton())
     steps, pulse = 10, _pulse(16 * dt)
-    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=1e9, stress_floor=0.0, seed=3)
+    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=None, stress_floor=1.0, seed=3)
     gated = RNOPoints(_untrained_rno(), bar.points, (-1.0, -1.0), rve, SETTINGS, fallback_capacity=bar.points,
                       precision=64, judge=judge)  # fmt: skip
     ExplicitFE2(bar, gated, dt, pulse).run(steps)
     assert judge.judge_steps == steps and judge.error < 1e-10
     # surrogate answers, judged against independent direct RVEs along the same histories
-    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=1e9, stress_floor=0.0, seed=3)
+    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=None, stress_floor=1.0, seed=3)
     free = RNOPoints(_untrained_rno(), bar.points, (1e30, 1e30), rve, SETTINGS, fallback_capacity=bar.points,
                      precision=64, judge=judge)  # fmt: skip
     fe2 = ExplicitFE2(bar, free, dt, pulse)
@@ -259,7 +259,7 @@ def test_judge_measures_the_delivered_stress_against_direct_rves() -> None:
     assert judge.error == pytest.approx((err2 / ref2) ** 0.5, rel=1e-9)
     assert judge.error > 0.05 and free.escalations == 0
     # a threshold below that error escalates the sampled points to the fallback pool
-    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=0.05, stress_floor=0.0, seed=3)
+    judge = SurrogateJudge(rve, bar.points, SETTINGS, sample=8, every=1, threshold=0.05, stress_floor=1.0, seed=3)
     esc = RNOPoints(_untrained_rno(), bar.points, (1e30, 1e30), rve, SETTINGS, fallback_capacity=bar.points,
                     precision=64, judge=judge)  # fmt: skip
     fe2 = ExplicitFE2(bar, esc, dt, pulse)
