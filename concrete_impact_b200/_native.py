@@ -126,6 +126,7 @@ class RVEBatchC(ctypes.Structure):
         ("tflag", ctypes.c_void_p),
         ("fe", ctypes.c_void_p),
         ("de", ctypes.c_void_p),
+        ("point_stride", ctypes.c_int64),
     ]
 
 

@@ -181,6 +181,9 @@ struct RveResponseArgs {
 // ---------------------------------------------------------------------------------------
 // Host-side argument builders from the public batch struct (shared by the C entry points).
 
+// Gauss points per SoA row: the whole batch's, also for a view of its first RVEs.
+inline int64_t rve_point_stride(const cib_rve_batch& b) { return b.point_stride > 0 ? b.point_stride : 8 * b.nelem; }
+
 template <typename T>
 inline PhaseTable<T> rve_phase_table(const cib_rve_batch& b) {
   PhaseTable<T> t;
@@ -220,7 +223,7 @@ inline RveResidualArgs<T> rve_residual_args(const cib_rve_batch& b, const double
   a.dw = dw;
   a.alpha = alpha;
   a.active = active;
-  a.ngp = 8 * b.nelem;
+  a.ngp = rve_point_stride(b);
   a.ep_n = static_cast<const T*>(b.plastic_strain_n);
   a.q_n = b.eqps_n;
   a.vpm_n = b.vpm_n;
@@ -268,7 +271,7 @@ inline RvePcgArgs<T> rve_pcg_args(const cib_rve_batch& b, const int32_t* sys_rve
   a.desc = reinterpret_cast<const RveDesc*>(b.desc);
   a.phase = b.phase;
   a.mats = rve_phase_table<T>(b);
-  a.ngp = 8 * b.nelem;
+  a.ngp = rve_point_stride(b);
   a.tparam = static_cast<const T*>(b.tparam);
   a.tflag = b.tflag;
   a.sys_rve = sys_rve;

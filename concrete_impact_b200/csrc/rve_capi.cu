@@ -41,8 +41,8 @@ int tangent_rhs_t(const cib_rve_batch& b, const int32_t* active, double* fe6, do
   a.desc = reinterpret_cast<const RveDesc*>(b.desc);
   a.phase = b.phase;
   a.mats = rve_phase_table<T>(b);
-  a.ngp = 8 * b.nelem;
-  a.ne_total = b.nelem;
+  a.ngp = rve_point_stride(b);
+  a.ne_total = rve_point_stride(b) / 8;
   a.tparam = static_cast<const T*>(b.tparam);
   a.tflag = b.tflag;
   a.active = active;
@@ -66,7 +66,7 @@ int response_t(const cib_rve_batch& b, const double* dt, const double* macro, co
   a.w = w;
   a.w_n = w_n;
   a.active = active;
-  a.ngp = 8 * b.nelem;
+  a.ngp = rve_point_stride(b);
   a.ep_n = static_cast<const T*>(b.plastic_strain_n);
   a.q_n = b.eqps_n;
   a.ep = static_cast<const T*>(b.plastic_strain);

@@ -103,7 +103,7 @@ int solve(const cib_rve_batch& b, int32_t nsys, const int32_t* sys_rve, const in
   a.desc = reinterpret_cast<const RveDesc*>(b.desc);
   a.phase = b.phase;
   a.mats = rve_phase_table<T>(b);
-  a.ngp = 8 * b.nelem;
+  a.ngp = rve_point_stride(b);
   a.tparam = static_cast<const T*>(b.tparam);
   a.tflag = b.tflag;
   a.sys_rve = sys_rve;

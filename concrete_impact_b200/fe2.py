@@ -155,6 +155,16 @@ class DirectRVEPoints:
             b.commit()
 
 
+def _pool_solver(model: StructuredHex8RVE):
+    """PCG controls of the small same-size RVE batches of the fallback pool and the judge:
+    a few hundred RVEs at most, so each system gets a cluster of CTAs (8 for an 8^3 RVE:
+    about 2.8x faster per solve than one CTA) instead of the size rule's one CTA."""
+    from .rve import LinearSolverOptions
+
+    nz = int(model.divisions[2])
+    return LinearSolverOptions(cluster=8 if nz >= 8 else (4 if nz >= 4 else 1))
+
+
 class SurrogateJudge:
     """Direct RVE solves that judge the surrogate's error during an FE^2 run.
 
@@ -183,7 +193,8 @@ class SurrogateJudge:
         self.every = max(int(every), 1)
         self.threshold = None if threshold is None else float(threshold)
         self.floor2 = float(stress_floor) ** 2
-        self.batch = RVEBatch([model] * pts.size, precision=precision, device_control=True)
+        self.batch = RVEBatch([model] * pts.size, precision=precision, device_control=True,
+                              linear_solver=_pool_solver(model))  # fmt: skip
         dev = self.batch.device
         self.points = torch.as_tensor(pts, device=dev)
         self.volume = float(self.batch.volumes[0])
@@ -266,7 +277,8 @@ class RNOPoints:
         self.flagged = torch.zeros(n_points, dtype=torch.bool, device=dev)
         self.slot_of = torch.full((n_points,), -1, dtype=torch.int64, device=dev)
         self.slots_used = 0
-        self.pool = (RVEBatch([model] * fallback_capacity, precision=precision, device_control=True)
+        self.pool = (RVEBatch([model] * fallback_capacity, precision=precision, device_control=True,
+                              linear_solver=_pool_solver(model))
                      if model is not None else None)  # fmt: skip
         self.capacity = fallback_capacity if model is not None else 0
         self.pool_points = torch.full((self.capacity,), -1, dtype=torch.int64, device=dev)

@@ -464,6 +464,7 @@ class RVEBatch:
         b.nrve = m
         b.nphase = len(self.phases)
         b.nelem = self.nelem if m == self.nrve else int(self.elem_offsets[m]) if m < self.nrve else self.nelem
+        b.point_stride = 8 * self.nelem  # the Gauss-point arrays keep the whole batch's layout
         b.precision = self.precision
         b.max_nxy = self.max_nxy
         b.desc = self.desc.data_ptr()

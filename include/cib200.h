@@ -280,6 +280,9 @@ typedef struct cib_rve_batch {
   /* element work arrays (caller-provided scratch) */
   double* fe;                   /* 24 * nelem: element nodal forces */
   double* de;                   /* 24 * nelem: element tangent diagonals */
+  /* SoA stride of the Gauss-point arrays; 0 = 8 * nelem.  A view of the first nrve RVEs of
+   * a larger batch (kernels launched over those RVEs only) keeps the larger batch's stride. */
+  int64_t point_stride;
 } cib_rve_batch;
 
 /* Fused residual pass (nonlinear_solid.py:428-493 + solver.py:88-100): for every Gauss
