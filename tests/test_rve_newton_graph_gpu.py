@@ -84,3 +84,29 @@ def test_graph_newton_raises_the_host_loops_maximum_iterations_error() -> None:
     assert errors[0].reason == errors[1].reason == "maximum_iterations_exceeded"
     assert errors[0].diagnostics["rve_index"] == errors[1].diagnostics["rve_index"]
     assert errors[0].diagnostics["iteration"] == errors[1].diagnostics["iteration"]
+
+
+@pytest.mark.parametrize("device_control", [False, True])
+def test_live_prefix_view_equals_a_batch_of_those_rves(device_control: bool) -> None:
+    """A live mask that covers the first RVEs launches the kernels over that prefix of the
+    batch; the states of those RVEs must be those of a batch holding only them (the
+    Gauss-point arrays keep the whole batch's stride)."""
+    models = [concrete_rve(e, 30 + i, 64) for i, e in enumerate(EDGES)]
+    paths = [random_strain_path(7000 + i, 40, 3, 8.0e-3, (10.0, 100.0)) for i in range(len(models))]
+    live = np.array([True, True, True, False, False])
+    results = []
+    for subset, mask in ((models[:3], None), (models, live)):
+        batch = R.RVEBatch(subset, precision=64, linear_solver=R.LinearSolverOptions(cluster=4),
+                           device_control=device_control)  # fmt: skip
+        n = len(subset)
+        vol = torch.as_tensor(batch.volumes, device=batch.device)[:, None]
+        out = []
+        for a, b in ((0, 8), (8, 16)):
+            batch.macro.copy_(torch.as_tensor(np.stack([p[1][b] for p in paths[:n]]), device=batch.device))
+            batch.dt.copy_(torch.as_tensor([p[0][b] - p[0][a] for p in paths[:n]], device=batch.device))
+            R.solve_batch_step(batch, batch.models[0].newton_settings, UPDATE, False, live_mask=mask)
+            batch.response(batch.batch_struct(UPDATE), batch.w, None, None)
+            out.append((batch.sums[:3, R.RS_SIGMA : R.RS_SIGMA + 6] / vol[:3]).cpu().numpy())
+            batch.commit()
+        results.append(np.asarray(out))
+    np.testing.assert_allclose(results[1], results[0], rtol=1e-12, atol=1e-12 * np.abs(results[0]).max())
