@@ -353,6 +353,19 @@ def _fe2_cpu(solves: int = 3) -> dict:
                       f"per step / {cores} cores"}  # fmt: skip
 
 
+def _rno_inference_line(inf: dict, peak: float, kind: str) -> dict:
+    """The trained surrogate's fused inference step at the 131,072 Gauss points of the
+    64 x 16 x 16 macro bar (one persistent rno_window_forward launch per step)."""
+    seconds = inf["ms_per_step"] / 1e3
+    achieved = inf["flop_per_step"] / seconds / 1e12
+    return {"points": inf["points"], "ms_per_step": inf["ms_per_step"], "points_per_s": inf["points"] / seconds,
+            "steps_timed": inf["steps"], "launches": inf["launches"],
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "peak_kind": f"{kind} (cuBLAS bf16, burst)",
+                         "note": "73,216 FLOP per point-step (unpadded MLP); the bias + exact-GELU epilogue on "
+                                 "CUDA cores bounds the step"}}  # fmt: skip
+
+
 def run_rno_train(args: argparse.Namespace) -> None:
     import torch
 
@@ -386,6 +399,7 @@ def run_rno_train(args: argparse.Namespace) -> None:
                                "kernel": "rno_window_forward/backward + split-K weight-gradient GEMMs",
                                "note": "219,648 FLOP per path-step; the time recursion leaves B/128 CTAs per step"},
                   "gpu_launches": out["launches"],
+                  "inference": _rno_inference_line(out["inference"], peak, kind),
                   "e2e": {"value": value, "unit": "path-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
                           "path": "device-resident dataset; one loss read-back per epoch"},
                   "clocks": clocks.summary(), "cpu_baseline": None if args.no_cpu_baseline else _rno_train_cpu()})  # fmt: skip

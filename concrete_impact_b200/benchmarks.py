@@ -280,7 +280,33 @@ def rno_training_workload(paths: int = 2000, steps: int = 200, epochs: int = 300
                 "loss_last": history[-1], "error_trained": relative_stress_error(rno.rollout(val), target),
                 "flop": path_steps * RNO_TRAIN_FLOP, "model": rno,
                 "launches": per_window * epochs * batches * (steps // c.tbptt_steps)})  # fmt: skip
+    out["inference"] = rno_inference_workload(rno)
     return out
+
+
+def rno_inference_workload(rno, points: int = 131072, steps: int = 50, warmup: int = 3) -> dict:
+    """Surrogate inference at ``points`` macro points (the 64 x 16 x 16 bar's Gauss points):
+    ``steps`` chained fused steps (latent carried from step to step) on seeded normalised
+    inputs, CUDA-event timed; one launch per step."""
+    g = torch.Generator(device="cuda").manual_seed(11)
+    strain = torch.randn((points, 6), generator=g, device="cuda", dtype=torch.float32)
+    rate = torch.randn((points, 6), generator=g, device="cuda", dtype=torch.float32)
+    coef = torch.full((points,), 0.01, dtype=torch.float32, device="cuda")
+    z = torch.zeros((2, points, 6), dtype=torch.float32, device="cuda")
+    stress = torch.empty((points, 6), dtype=torch.float32, device="cuda")
+
+    def step() -> None:
+        rno.predict_normalized(strain, rate, coef, z, stress)
+        z[0].copy_(z[1])
+
+    for _ in range(warmup):
+        step()
+    calls0 = _native.LAUNCHED[0]
+    ms = _elapsed_ms(lambda: [step() for _ in range(steps)])
+    if int(rno.err.item()) != 0:
+        raise RuntimeError("a tensor-core wait timed out in the surrogate inference kernel")
+    return {"ms_per_step": ms / steps, "points": points, "steps": steps, "launches": _native.LAUNCHED[0] - calls0,
+            "flop_per_step": points * RNO_FORWARD_FLOP}  # fmt: skip
 
 
 # ---------------------------------------------------------------------------------------

@@ -4,9 +4,11 @@
 // C[M x N] = A[M x K] . B[N x K]^T with A, B bf16 row-major (K contiguous), fp32 accumulation
 // in tensor memory.  One CTA computes a 128-row tile over the full N (16..128, multiple of
 // 16) and a K range (split-K over gridDim.y).  Operands are staged in shared memory in the
-// K-major, no-swizzle canonical layout of tcgen05 (8-row x 16-byte core matrices); one
-// elected thread issues tcgen05.mma (M = 128, N, K = 16 per instruction) and commits to an
-// mbarrier; every wait is bounded in time and reports through an error word.  The epilogue
+// K-major, no-swizzle canonical layout of tcgen05 (8-row x 16-byte core matrices) by
+// cp.async through a three-slot pipeline, so that the copies of the next two K chunks
+// overlap the MMA of the current one; one elected thread issues tcgen05.mma (M = 128, N,
+// K = 16 per instruction) and commits each chunk to its slot's mbarrier; every wait is
+// bounded in time and reports through an error word.  The epilogue
 // reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows)
 // and applies one of:
 //   EPI_F32        C = acc                                   (fp32 out)
@@ -26,6 +28,7 @@ namespace {
 
 constexpr int GEMM_THREADS = 128;
 constexpr int KC = 64;  // K elements staged per chunk
+constexpr int GEMM_STAGES = 3;  // shared-memory slots of the copy/MMA pipeline
 
 enum Epi { EPI_F32 = 0, EPI_BIAS_F32 = 1, EPI_BIAS_GELU = 2, EPI_GELU_BWD = 3, EPI_PARTIAL = 4 };
 
@@ -51,60 +54,81 @@ struct GemmArgs {
 
 using namespace umma;
 
+// 16-byte asynchronous global->shared copy; src_bytes 0 fills the 16 bytes with zeros.
+__device__ __forceinline__ void cp_async16(uint8_t* dst, const void* src, bool pred) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(pred ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
+struct __align__(1024) GemmSmem {
+  uint8_t a[GEMM_STAGES][128 * KC * 2];
+  uint8_t b[GEMM_STAGES][128 * KC * 2];
+  uint64_t bar[GEMM_STAGES];
+  uint32_t tmem_base;
+};
+
 template <int EPI>
 __global__ void __launch_bounds__(GEMM_THREADS) umma_gemm_kernel(const GemmArgs a) {
-  __shared__ __align__(1024) uint8_t sA[128 * KC * 2];
-  __shared__ __align__(1024) uint8_t sB[128 * KC * 2];
-  __shared__ __align__(8) uint64_t mbar;
-  __shared__ uint32_t tmem_base;
-  __shared__ int failed;
+  extern __shared__ uint8_t smem_raw[];
+  GemmSmem& S = *reinterpret_cast<GemmSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * 128;
   const int k_begin = blockIdx.y * a.k_per_split;
   const int k_end = min(a.K, k_begin + a.k_per_split);
+  const int chunks = k_end > k_begin ? (k_end - k_begin + KC - 1) / KC : 0;
   const uint32_t ncols = a.N <= 32 ? 32u : (a.N <= 64 ? 64u : 128u);
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
-                 "r"(ncols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
-    failed = 0;
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  if (warp == 0) tmem_alloc(&S.tmem_base, ncols);
+  if (tid == 0)
+    for (int s = 0; s < GEMM_STAGES; ++s) mbar_init(&S.bar[s], 1);
+  fence_before_sync();
   __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem = tmem_base;
+  fence_after_sync();
+  const uint32_t tmem = S.tmem_base;
   const uint32_t idesc = idesc_bf16(a.N);
-  uint32_t phase = 0;
-  int chunks = 0;
-  for (int k0 = k_begin; k0 < k_end; k0 += KC) {
-    // stage A (128 x KC) and B (N x KC) chunks, zero-filled outside the matrices
+
+  // stage chunk i (A: 128 x KC, B: N x KC) into slot st with cp.async, zero-filled outside
+  // the matrices and the K range
+  auto load_chunk = [&](int i, int st) {
+    const int k0 = k_begin + i * KC;
     for (int v = tid; v < 128 * (KC / 8); v += GEMM_THREADS) {
       const int r = v / (KC / 8), c = (v % (KC / 8)) * 8;
-      uint4 val = make_uint4(0, 0, 0, 0);
-      if (m0 + r < a.M && k0 + c < k_end)
-        val = *reinterpret_cast<const uint4*>(a.A + (size_t)(m0 + r) * a.lda + k0 + c);
-      *reinterpret_cast<uint4*>(sA + core_offset(r, c, KC)) = val;
+      const bool in = m0 + r < a.M && k0 + c < k_end;
+      cp_async16(S.a[st] + core_offset(r, c, KC), in ? a.A + (size_t)(m0 + r) * a.lda + k0 + c : a.A, in);
     }
     for (int v = tid; v < a.N * (KC / 8); v += GEMM_THREADS) {
       const int r = v / (KC / 8), c = (v % (KC / 8)) * 8;
-      uint4 val = make_uint4(0, 0, 0, 0);
-      if (k0 + c < k_end) val = *reinterpret_cast<const uint4*>(a.B + (size_t)r * a.ldb + k0 + c);
-      *reinterpret_cast<uint4*>(sB + core_offset(r, c, KC)) = val;
+      const bool in = k0 + c < k_end;
+      cp_async16(S.b[st] + core_offset(r, c, KC), in ? a.B + (size_t)r * a.ldb + k0 + c : a.B, in);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
+  };
+
+  // Pipeline: GEMM_STAGES - 1 chunks in flight ahead of the MMA.  Chunk i lands in slot
+  // i % GEMM_STAGES; the slot is refilled (with chunk i + GEMM_STAGES - 1) once the MMA of
+  // chunk i - 1 that read it has completed, while the MMA of chunk i runs.
+#pragma unroll
+  for (int s = 0; s < GEMM_STAGES - 1; ++s) {
+    if (s < chunks) load_chunk(s, s);
+    cp_async_commit();
+  }
+  bool failed = false;
+  for (int i = 0; i < chunks; ++i) {
+    const int st = i % GEMM_STAGES;
+    cp_async_wait<GEMM_STAGES - 2>();  // chunk i's group has landed (this thread's copies)
+    fence_smem_to_async();
+    __syncthreads();  // ... and every thread's
     if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int steps = min(KC, k_end - k0) / 16;
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+      fence_after_sync();
+      const int steps = min(KC, k_end - (k_begin + i * KC)) / 16;
+      const uint32_t a0 = smem_u32(S.a[st]), b0 = smem_u32(S.b[st]);
       for (int s = 0; s < steps; ++s) {
         const uint64_t da = sdesc(a0 + 256 * s, 128, KC * 16);
         const uint64_t db = sdesc(b0 + 256 * s, 128, KC * 16);
-        const uint32_t acc = (chunks > 0 || s > 0) ? 1u : 0u;
+        const uint32_t acc = (i > 0 || s > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
@@ -112,17 +136,30 @@ __global__ void __launch_bounds__(GEMM_THREADS) umma_gemm_kernel(const GemmArgs 
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&mbar))
+                       smem_u32(&S.bar[st]))
                    : "memory");
     }
-    if (!mbar_wait(&mbar, phase)) {
-      failed = 1;
+    const int j = i + GEMM_STAGES - 1;
+    if (j < chunks) {
+      if (i >= 1) {
+        const int prev = i - 1;
+        const bool ok = mbar_wait(&S.bar[prev % GEMM_STAGES], (uint32_t)((prev / GEMM_STAGES) & 1));
+        if (__syncthreads_or(ok ? 0 : 1)) {
+          failed = true;
+          break;
+        }
+      }
+      load_chunk(j, j % GEMM_STAGES);
     }
-    phase ^= 1u;
-    ++chunks;
-    __syncthreads();
-    if (failed) break;
+    cp_async_commit();
   }
+  // the last commit covers every MMA issued before it
+  if (!failed && chunks > 0) {
+    const int last = chunks - 1;
+    const bool ok = mbar_wait(&S.bar[last % GEMM_STAGES], (uint32_t)((last / GEMM_STAGES) & 1));
+    failed = __syncthreads_or(ok ? 0 : 1) != 0;
+  }
+  cp_async_wait<0>();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (failed) {
     if (tid == 0 && a.err) atomicExch(a.err, 1u);
@@ -244,12 +281,19 @@ extern "C" int cib_mlp_gemm(int32_t epilogue, int32_t M, int32_t N, int32_t K, c
   }
   const dim3 grid((unsigned)((M + 127) / 128), (unsigned)ny);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int bytes = (int)sizeof(GemmSmem);
+  const void* kernels[5] = {reinterpret_cast<const void*>(umma_gemm_kernel<EPI_F32>),
+                            reinterpret_cast<const void*>(umma_gemm_kernel<EPI_BIAS_F32>),
+                            reinterpret_cast<const void*>(umma_gemm_kernel<EPI_BIAS_GELU>),
+                            reinterpret_cast<const void*>(umma_gemm_kernel<EPI_GELU_BWD>),
+                            reinterpret_cast<const void*>(umma_gemm_kernel<EPI_PARTIAL>)};
+  if (allow_dynamic_smem(kernels[epilogue], bytes) != CIB_OK) return CIB_ECUDA;
   switch (epilogue) {
-    case EPI_F32: umma_gemm_kernel<EPI_F32><<<grid, GEMM_THREADS, 0, st>>>(a); break;
-    case EPI_BIAS_F32: umma_gemm_kernel<EPI_BIAS_F32><<<grid, GEMM_THREADS, 0, st>>>(a); break;
-    case EPI_BIAS_GELU: umma_gemm_kernel<EPI_BIAS_GELU><<<grid, GEMM_THREADS, 0, st>>>(a); break;
-    case EPI_GELU_BWD: umma_gemm_kernel<EPI_GELU_BWD><<<grid, GEMM_THREADS, 0, st>>>(a); break;
-    default: umma_gemm_kernel<EPI_PARTIAL><<<grid, GEMM_THREADS, 0, st>>>(a); break;
+    case EPI_F32: umma_gemm_kernel<EPI_F32><<<grid, GEMM_THREADS, bytes, st>>>(a); break;
+    case EPI_BIAS_F32: umma_gemm_kernel<EPI_BIAS_F32><<<grid, GEMM_THREADS, bytes, st>>>(a); break;
+    case EPI_BIAS_GELU: umma_gemm_kernel<EPI_BIAS_GELU><<<grid, GEMM_THREADS, bytes, st>>>(a); break;
+    case EPI_GELU_BWD: umma_gemm_kernel<EPI_GELU_BWD><<<grid, GEMM_THREADS, bytes, st>>>(a); break;
+    default: umma_gemm_kernel<EPI_PARTIAL><<<grid, GEMM_THREADS, bytes, st>>>(a); break;
   }
   return check_launch();
 }

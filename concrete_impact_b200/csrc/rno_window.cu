@@ -9,7 +9,9 @@
 // epilogue is the step's critical path: 16 warps (four per TMEM lane quarter, each on a
 // quarter of the columns) share it.
 // The paths of a window are independent in time, so the recurrence needs no grid-wide
-// synchronisation.
+// synchronisation.  The forward kernel is persistent: one CTA per SM stages the weights
+// once and runs its 128-path tiles one after another (a 131,072-point inference step is
+// 1,024 tiles on 148 CTAs).
 //
 // Per step t and path p (normalised units; x = [strain, rate, z] padded to 32 bf16):
 //   Z_l = H_{l-1} W_l^T + b_l, H_l = gelu(Z_l) (bf16), l = 1..3;  Y = H_3 W_4^T + b_4
@@ -25,6 +27,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "cib200.h"
 #include "cib_common.cuh"
@@ -112,8 +116,7 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
   const int quarter = warp & 3, group = warp >> 2;
   const int row = quarter * 32 + lane;
   const int B = w.B, T = w.T;
-  const int p = blockIdx.x * TILE + row;
-  const bool valid = p < B;
+  const int ntiles = (B + TILE - 1) / TILE;
   const size_t R = w.ldt > 0 ? (size_t)w.ldt : (size_t)B * T;
 
   stage_matrix(S.w1, static_cast<const __nv_bfloat16*>(w.W[0]), HID, XIN, XIN);
@@ -131,147 +134,152 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_forward_kernel(const
   const uint32_t tmem = S.tmem;
   const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
   const bool has_skip = w.skip != nullptr;
-
-  float z[6] = {0, 0, 0, 0, 0, 0};
-  if (group == 0 && valid)
-#pragma unroll
-    for (int k = 0; k < 6; ++k) z[k] = w.z[(size_t)p * 6 + k];
-  double sq = 0.0;
   uint32_t phase = 0;
   bool ok = true;
-  // inputs of the next step, loaded one step ahead so that their latency hides behind
-  // the current step's layers
-  float ne[6] = {0, 0, 0, 0, 0, 0}, nr[6] = {0, 0, 0, 0, 0, 0}, nt[6] = {0, 0, 0, 0, 0, 0}, nc = 0.0f;
-  if (group == 0 && valid) {
+
+  // persistent over 128-path tiles: the weights are staged once per CTA
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int p = tile * TILE + row;
+    const bool valid = p < B;
+    float z[6] = {0, 0, 0, 0, 0, 0};
+    if (group == 0 && valid)
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      ne[k] = w.strain[(size_t)p * 6 + k];
-      nr[k] = w.rate[(size_t)p * 6 + k];
-      if (w.target) nt[k] = w.target[(size_t)p * 6 + k];
+      for (int k = 0; k < 6; ++k) z[k] = w.z[(size_t)p * 6 + k];
+    double sq = 0.0;
+    // inputs of the next step, loaded one step ahead so that their latency hides behind
+    // the current step's layers
+    float ne[6] = {0, 0, 0, 0, 0, 0}, nr[6] = {0, 0, 0, 0, 0, 0}, nt[6] = {0, 0, 0, 0, 0, 0}, nc = 0.0f;
+    if (group == 0 && valid) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        ne[k] = w.strain[(size_t)p * 6 + k];
+        nr[k] = w.rate[(size_t)p * 6 + k];
+        if (w.target) nt[k] = w.target[(size_t)p * 6 + k];
+      }
+      nc = w.coef[p];
     }
-    nc = w.coef[p];
-  }
-  for (int t = 0; t < T && ok; ++t) {
-    const size_t g = (size_t)t * B + p;  // (t, p) row of the window
-    float e[6], tg[6];
-    const float c = nc;
+    for (int t = 0; t < T && ok; ++t) {
+      const size_t g = (size_t)t * B + p;  // (t, p) row of the window
+      float e[6], tg[6];
+      const float c = nc;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      e[k] = ne[k];
-      tg[k] = nt[k];
-    }
-    if (group == 0) {
-      float xin[XIN];
+      for (int k = 0; k < 6; ++k) {
+        e[k] = ne[k];
+        tg[k] = nt[k];
+      }
+      if (group == 0) {
+        float xin[XIN];
 #pragma unroll
-      for (int c2 = 0; c2 < XIN; ++c2) xin[c2] = 0.0f;
-      if (valid) {
+        for (int c2 = 0; c2 < XIN; ++c2) xin[c2] = 0.0f;
+        if (valid) {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          xin[k] = e[k];
-          xin[6 + k] = nr[k];
-          xin[12 + k] = z[k];
+          for (int k = 0; k < 6; ++k) {
+            xin[k] = e[k];
+            xin[6 + k] = nr[k];
+            xin[12 + k] = z[k];
+          }
+        }
+        if (valid && t + 1 < T) {
+          const size_t gn = g + (size_t)B;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            ne[k] = w.strain[gn * 6 + k];
+            nr[k] = w.rate[gn * 6 + k];
+            if (w.target) nt[k] = w.target[gn * 6 + k];
+          }
+          nc = w.coef[gn];
+        }
+#pragma unroll
+        for (int c = 0; c < XIN; c += 8) put8(S.x, row, c, XIN, xin + c);
+        if (w.Xt && valid) {
+          __nv_bfloat16* xt = static_cast<__nv_bfloat16*>(w.Xt);
+#pragma unroll
+          for (int c = 0; c < XIN; ++c) xt[(size_t)c * R + g] = __float2bfloat16_rn(xin[c]);
         }
       }
-      if (valid && t + 1 < T) {
-        const size_t gn = g + (size_t)B;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          ne[k] = w.strain[gn * 6 + k];
-          nr[k] = w.rate[gn * 6 + k];
-          if (w.target) nt[k] = w.target[gn * 6 + k];
-        }
-        nc = w.coef[gn];
-      }
-#pragma unroll
-      for (int c = 0; c < XIN; c += 8) put8(S.x, row, c, XIN, xin + c);
-      if (w.Xt && valid) {
-        __nv_bfloat16* xt = static_cast<__nv_bfloat16*>(w.Xt);
-#pragma unroll
-        for (int c = 0; c < XIN; ++c) xt[(size_t)c * R + g] = __float2bfloat16_rn(xin[c]);
-      }
-    }
-    // hidden layers
-    for (int l = 0; l < 3 && ok; ++l) {
-      ok = run_layer(&S.bar, tmem, l == 0 ? S.x : S.h, l == 0 ? S.w1 : (l == 1 ? S.w2 : S.w3), l == 0 ? XIN : HID,
-                     HID, phase);
-      if (!ok) break;
-      float* Zl = w.Z[l];
-      __nv_bfloat16* Ht = static_cast<__nv_bfloat16*>(w.Ht[l]);
+      // hidden layers
+      for (int l = 0; l < 3 && ok; ++l) {
+        ok = run_layer(&S.bar, tmem, l == 0 ? S.x : S.h, l == 0 ? S.w1 : (l == 1 ? S.w2 : S.w3), l == 0 ? XIN : HID,
+                       HID, phase);
+        if (!ok) break;
+        float* Zl = w.Z[l];
+        __nv_bfloat16* Ht = static_cast<__nv_bfloat16*>(w.Ht[l]);
 #pragma unroll 1
-      for (int cb = 0; cb < GROUP_CHUNKS; ++cb) {
-        const int c0 = GROUP_COLS * group + 16 * cb;
+        for (int cb = 0; cb < GROUP_CHUNKS; ++cb) {
+          const int c0 = GROUP_COLS * group + 16 * cb;
+          float v[16];
+          tmem_ld16(lane_addr + (uint32_t)c0, v);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] += S.bias[l * HID + c0 + j];
+          if (Zl && valid) {
+            float4* dst = reinterpret_cast<float4*>(Zl + g * HID + c0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = gelu(v[j]);
+          put8(S.h, row, c0, HID, v);
+          put8(S.h, row, c0 + 8, HID, v + 8);
+          if (Ht && valid)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) Ht[(size_t)(c0 + j) * R + g] = __float2bfloat16_rn(v[j]);
+        }
+      }
+      if (!ok) break;
+      // output layer and latent update
+      ok = run_layer(&S.bar, tmem, S.h, S.w4, HID, YOUT, phase);
+      if (!ok) break;
+      if (group == 0) {
         float v[16];
-        tmem_ld16(lane_addr + (uint32_t)c0, v);
+        tmem_ld16(lane_addr, v);
+        if (valid) {
+          float s[6];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] += S.bias[l * HID + c0 + j];
-        if (Zl && valid) {
-          float4* dst = reinterpret_cast<float4*>(Zl + g * HID + c0);
+          for (int k = 0; k < 6; ++k) s[k] = v[k] + S.bias[3 * HID + k];
+          if (has_skip) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-        }
+            for (int k = 0; k < 6; ++k) {
+              float acc = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = gelu(v[j]);
-        put8(S.h, row, c0, HID, v);
-        put8(S.h, row, c0 + 8, HID, v + 8);
-        if (Ht && valid)
+              for (int j = 0; j < 6; ++j) acc += S.skip[6 * k + j] * (e[j] - z[j]);
+              s[k] += acc;
+            }
+          }
+          if (w.stress)
 #pragma unroll
-          for (int j = 0; j < 16; ++j) Ht[(size_t)(c0 + j) * R + g] = __float2bfloat16_rn(v[j]);
-      }
-    }
-    if (!ok) break;
-    // output layer and latent update
-    ok = run_layer(&S.bar, tmem, S.h, S.w4, HID, YOUT, phase);
-    if (!ok) break;
-    if (group == 0) {
-      float v[16];
-      tmem_ld16(lane_addr, v);
-      if (valid) {
-        float s[6];
+            for (int k = 0; k < 6; ++k) w.stress[g * 6 + k] = s[k];
+          if (w.target) {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) s[k] = v[k] + S.bias[3 * HID + k];
-        if (has_skip) {
+            for (int k = 0; k < 6; ++k) {
+              const float d = s[k] - tg[k];
+              sq += (double)d * d;
+              if (w.gS) w.gS[g * 6 + k] = w.loss_scale * 2.0f * d;
+            }
+          }
+          float* zn = w.z + (size_t)(t + 1) * B * 6 + (size_t)p * 6;
 #pragma unroll
           for (int k = 0; k < 6; ++k) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int j = 0; j < 6; ++j) acc += S.skip[6 * k + j] * (e[j] - z[j]);
-            s[k] += acc;
+            z[k] = z[k] + c * (v[6 + k] + S.bias[3 * HID + 6 + k]);
+            zn[k] = z[k];
           }
-        }
-        if (w.stress)
-#pragma unroll
-          for (int k = 0; k < 6; ++k) w.stress[g * 6 + k] = s[k];
-        if (w.target) {
-#pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            const float d = s[k] - tg[k];
-            sq += (double)d * d;
-            if (w.gS) w.gS[g * 6 + k] = w.loss_scale * 2.0f * d;
-          }
-        }
-        float* zn = w.z + (size_t)(t + 1) * B * 6 + (size_t)p * 6;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-          z[k] = z[k] + c * (v[6 + k] + S.bias[3 * HID + 6 + k]);
-          zn[k] = z[k];
         }
       }
     }
-  }
+    // window loss partial of this tile (first row of loss_part; the others zero)
+    if (w.loss_part && ok) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+      if (lane == 0) S.red[warp] = sq;
+      __syncthreads();
+      if (tid == 0) {
+        double tot = 0.0;
+        for (int i = 0; i < RW_THREADS / 32; ++i) tot += S.red[i];
+        w.loss_part[tile] = tot;
+        for (int t = 1; t < T; ++t) w.loss_part[(size_t)t * ntiles + tile] = 0.0;
+      }
+    }
+  }  // tile
   if (!ok && tid == 0 && w.err) atomicExch(w.err, 1u);
-  // window loss partial of this CTA (first row of loss_part; the others zero)
-  if (w.loss_part) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-    if (lane == 0) S.red[warp] = sq;
-    __syncthreads();
-    if (tid == 0) {
-      double tot = 0.0;
-      for (int i = 0; i < RW_THREADS / 32; ++i) tot += S.red[i];
-      w.loss_part[blockIdx.x] = tot;
-      for (int t = 1; t < T; ++t) w.loss_part[(size_t)t * gridDim.x + blockIdx.x] = 0.0;
-    }
-  }
   fence_before_sync();
   __syncthreads();
   if (warp == 0) {
@@ -434,7 +442,8 @@ extern "C" int cib_rno_window_forward(const cib_rno_window* w, void* stream) {
   const size_t bytes = sizeof(FwdSmem);
   if (allow_dynamic_smem(reinterpret_cast<const void*>(rno_window_forward_kernel), (int)bytes) != CIB_OK)
     return CIB_ECUDA;
-  const unsigned grid = (unsigned)((w->B + TILE - 1) / TILE);
+  // one CTA per SM (the staged weights fill most of its shared memory), each looping over tiles
+  const unsigned grid = (unsigned)std::min<int64_t>((w->B + TILE - 1) / TILE, sm_count());
   rno_window_forward_kernel<<<grid, RW_THREADS, bytes, reinterpret_cast<cudaStream_t>(stream)>>>(*w);
   return check_launch();
 }

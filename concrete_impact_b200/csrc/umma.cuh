@@ -118,11 +118,23 @@ __device__ __forceinline__ float gelu_grad(float x) {
 }
 
 // Copy a row-major bf16 matrix (rows x k, leading dimension ld) into the canonical layout.
+// Each thread issues four 16-byte loads before its stores, so that the copy waits on the
+// memory latency once per four chunks instead of once per chunk.
 __device__ __forceinline__ void stage_matrix(uint8_t* dst, const __nv_bfloat16* src, int rows, int k, int ld) {
-  const int chunks = k / 8;
-  for (int v = threadIdx.x; v < rows * chunks; v += blockDim.x) {
-    const int r = v / chunks, c = (v % chunks) * 8;
-    *reinterpret_cast<uint4*>(dst + core_offset(r, c, k)) = *reinterpret_cast<const uint4*>(src + (size_t)r * ld + c);
+  constexpr int U = 4;
+  const int chunks = k / 8, total = rows * chunks;
+  for (int base = threadIdx.x; base < total; base += U * blockDim.x) {
+    uint4 q[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int v = base + u * (int)blockDim.x;
+      if (v < total) q[u] = *reinterpret_cast<const uint4*>(src + (size_t)(v / chunks) * ld + (v % chunks) * 8);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int v = base + u * (int)blockDim.x;
+      if (v < total) *reinterpret_cast<uint4*>(dst + core_offset(v / chunks, (v % chunks) * 8, k)) = q[u];
+    }
   }
 }
 

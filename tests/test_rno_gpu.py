@@ -132,6 +132,27 @@ def test_fused_predict_and_rollout_match_unfused() -> None:
     assert _rel(rf.cpu(), rp.cpu()) < 1e-4
 
 
+def test_persistent_forward_runs_more_tiles_than_ctas() -> None:
+    """The forward window kernel runs one CTA per SM over 128-path tiles: a ragged batch of
+    313 tiles (more than one per CTA) gives the per-step GEMM path's stresses, latents and
+    per-tile window loss."""
+    T, B = 2, 40_000
+    fused, plain = RNOSurrogate(RNOConfig(seed=8)), RNOSurrogate(RNOConfig(seed=8))
+    plain.fused = False
+    window = _window(T, B, 9)
+    for m in (fused, plain):
+        m.load_window(*window)
+        m.window_step(T, B, train=False)
+    torch.cuda.synchronize()
+    assert int(fused.err.item()) == 0 and int(plain.err.item()) == 0
+    assert fused.window_loss() == pytest.approx(plain.window_loss(), rel=1e-5)
+    assert _rel(fused._window["z"].cpu(), plain._window["z"].cpu()) < 1e-5
+    strain, rate, _, coef, z0 = window
+    sf, zf, _ = fused.predict(strain[0], rate[0], z0, coef[0])
+    sp, zp, _ = plain.predict(strain[0], rate[0], z0, coef[0])
+    assert _rel(sf.cpu(), sp.cpu()) < 1e-5 and _rel(zf.cpu(), zp.cpu()) < 1e-5
+
+
 def test_training_divergence_guard_restores_finite_weights() -> None:
     data = _material_point_dataset(P=128, T=50, seed=13)
     scales = RNOScales.from_data(data.strain[:, 1:], data.rates(), data.stress[:, 1:])
