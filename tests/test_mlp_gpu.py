@@ -13,7 +13,9 @@ from concrete_impact_b200 import mlp
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(1, 16, 16), (100, 16, 32), (128, 128, 128), (512, 128, 32), (1000, 32, 128), (300, 128, 256), (257, 64, 80)]
+# the last two run the K pipeline through many slot reuses (65 and 128 chunks of 64)
+SHAPES = [(1, 16, 16), (100, 16, 32), (128, 128, 128), (512, 128, 32), (1000, 32, 128), (300, 128, 256), (257, 64, 80),
+          (129, 48, 4112), (256, 128, 8192)]
 
 
 def _rand(m: int, k: int, seed: int) -> torch.Tensor:
@@ -69,11 +71,11 @@ def test_gemm_gelu_forward_and_backward_epilogues(m: int, n: int, k: int) -> Non
     assert err.item() == 0
 
 
-def test_gemm_split_k_partials_reduce_to_the_product() -> None:
-    m, n, k = 128, 128, 2048
+@pytest.mark.parametrize("k,splits", [(2048, 8), (25600, 5)])
+def test_gemm_split_k_partials_reduce_to_the_product(k: int, splits: int) -> None:
+    m, n = 128, 128
     a, b = _rand(m, k, 5), _rand(n, k, 6)
     err = _err()
-    splits = 8
     partial = torch.empty((splits, m, n), device="cuda")
     mlp.gemm(mlp.EPI_PARTIAL, a, b, c=partial.view(splits * m, n), splits=splits, err=err)
     out = torch.empty((m, n), device="cuda")
