@@ -418,6 +418,19 @@ def _progress(stage: str, seconds: float, payload: dict) -> None:
     sys.stderr.flush()
 
 
+def _fe2_roofline(steps_per_s: float) -> dict:
+    """Surrogate FLOPs of a macro step (131,072 points x the MLP's 73,216) over the whole
+    step's time, against the bf16 tensor peak."""
+    from concrete_impact_b200.benchmarks import RNO_FORWARD_FLOP
+
+    peak, kind = _tensor_peak()
+    achieved = steps_per_s * 131072 * RNO_FORWARD_FLOP / 1e12
+    return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None, "peak_kind": f"{kind} (cuBLAS bf16, burst)",
+            "note": "per step: one persistent fused surrogate launch (1,024 tiles of 128 points on one CTA per SM), "
+                    "the gate kernels, and the macro Hex8 and Verlet kernels; time is the whole step's"}
+
+
 def run_fe2(args: argparse.Namespace) -> None:
     """Train the surrogate (random + impact calibration paths), check it against all-direct
     FE^2 (FP64 RVEs) on a 64x2x2 bar, then time surrogate FE^2 on the 64x16x16 bar for
@@ -487,9 +500,7 @@ def run_fe2(args: argparse.Namespace) -> None:
                   "training": {**info, "recipe": recipe.__dict__, "envelope": envelope},
                   "gate": {"flagged_points": speed["flagged_points"], "fallback_steps": speed["fallback_steps"]},
                   "simulated_time_s": speed["simulated_time_s"],
-                  "roofline": {"bound": "tensor", "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
-                               "traffic": None, "note": "per step: one fused surrogate launch (T = 1, 1,024 CTAs) "
-                                                        "plus the macro Hex8 and Verlet kernels"},
+                  "roofline": _fe2_roofline(value),
                   "gpu_launches": speed["launches"],
                   "e2e": {"value": value, "unit": "macro steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                           "path": "ExplicitFE2.run on device-resident macro fields"},
