@@ -417,6 +417,170 @@ __global__ void __launch_bounds__(RW_THREADS, 1) rno_window_backward_kernel(cons
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Inference step (T = 1, nothing saved for a backward pass) over many tiles: the CTA's two
+// halves of 8 warps each run their own 128-path tile with their own operand tiles, TMEM
+// columns, mbarrier and named barrier, so that one half's bias/GELU epilogue overlaps the
+// other half's tensor-core layer instead of every warp waiting on each MMA.  The weights are
+// staged once per CTA and shared.  Same arithmetic per path as rno_window_forward_kernel
+// (the same results bit for bit).
+constexpr int INF_HALF = RW_THREADS / 2;       // threads of a half
+constexpr int INF_GROUP_COLS = 64;             // epilogue columns per warp (2 groups per quarter)
+
+struct __align__(1024) InfSmem {
+  uint8_t w1[HID * XIN * 2];
+  uint8_t w2[HID * HID * 2];
+  uint8_t w3[HID * HID * 2];
+  uint8_t w4[YOUT * HID * 2];
+  uint8_t x[2][TILE * XIN * 2];
+  uint8_t h[2][TILE * HID * 2];
+  float bias[3 * HID + YOUT];
+  float skip[36];
+  uint64_t bar[2];
+  uint32_t tmem;
+};
+
+// Named barrier of one half (ids 1 and 2; 0 is __syncthreads).
+__device__ __forceinline__ void half_sync(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(INF_HALF) : "memory");
+}
+// Same, returning whether any thread of the half passed a true flag.
+__device__ __forceinline__ bool half_sync_or(int id, bool flag) {
+  uint32_t out;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(out)
+      : "r"((uint32_t)flag), "r"(id), "n"(INF_HALF)
+      : "memory");
+  return out != 0;
+}
+
+// run_layer for one half: its first thread issues, the half waits on its own mbarrier.
+__device__ __forceinline__ bool run_layer_half(uint64_t* bar, uint32_t tmem, const uint8_t* a, const uint8_t* b, int k,
+                                               int n, uint32_t& phase, int id, bool issuer) {
+  fence_smem_to_async();
+  fence_before_sync();
+  half_sync(id);
+  if (issuer) {
+    fence_after_sync();
+    mma_bf16(tmem, smem_u32(a), smem_u32(b), k, n, false, bar);
+  }
+  const bool ok = mbar_wait(bar, phase);
+  phase ^= 1u;
+  fence_after_sync();
+  return !half_sync_or(id, !ok);
+}
+
+__global__ void __launch_bounds__(RW_THREADS, 1) rno_infer_kernel(const cib_rno_window w) {
+  extern __shared__ uint8_t smem_raw[];
+  InfSmem& S = *reinterpret_cast<InfSmem*>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int half = warp >> 3, quarter = warp & 3, group = (warp >> 2) & 1;
+  const int row = quarter * 32 + lane;
+  const int bar_id = 1 + half;
+  const bool issuer = (tid & (INF_HALF - 1)) == 0;
+  const int B = w.B;
+  const int ntiles = (B + TILE - 1) / TILE;
+
+  stage_matrix(S.w1, static_cast<const __nv_bfloat16*>(w.W[0]), HID, XIN, XIN);
+  stage_matrix(S.w2, static_cast<const __nv_bfloat16*>(w.W[1]), HID, HID, HID);
+  stage_matrix(S.w3, static_cast<const __nv_bfloat16*>(w.W[2]), HID, HID, HID);
+  stage_matrix(S.w4, static_cast<const __nv_bfloat16*>(w.W[3]), YOUT, HID, HID);
+  for (int i = tid; i < 3 * HID + YOUT; i += RW_THREADS) S.bias[i] = w.bias[i / HID < 3 ? i / HID : 3][i % HID];
+  for (int i = tid; i < 36; i += RW_THREADS) S.skip[i] = w.skip ? w.skip[i] : 0.0f;
+  if (warp == 0) tmem_alloc(&S.tmem, 2 * TMEM_COLS);
+  if (tid == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+  }
+  fence_smem_to_async();
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = S.tmem + (uint32_t)(half * TMEM_COLS);
+  const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+  const bool has_skip = w.skip != nullptr;
+  uint8_t* xs = S.x[half];
+  uint8_t* hs = S.h[half];
+  uint64_t* bar = &S.bar[half];
+  uint32_t phase = 0;
+  bool ok = true;
+
+  for (int tile = 2 * blockIdx.x + half; tile < ntiles && ok; tile += 2 * gridDim.x) {
+    const int p = tile * TILE + row;
+    const bool valid = p < B;
+    float z[6] = {0, 0, 0, 0, 0, 0}, e[6] = {0, 0, 0, 0, 0, 0};
+    float c = 0.0f;
+    if (group == 0) {
+      float xin[XIN];
+#pragma unroll
+      for (int c2 = 0; c2 < XIN; ++c2) xin[c2] = 0.0f;
+      if (valid) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          z[k] = w.z[(size_t)p * 6 + k];
+          e[k] = w.strain[(size_t)p * 6 + k];
+          xin[k] = e[k];
+          xin[6 + k] = w.rate[(size_t)p * 6 + k];
+          xin[12 + k] = z[k];
+        }
+        c = w.coef[p];
+      }
+#pragma unroll
+      for (int c2 = 0; c2 < XIN; c2 += 8) put8(xs, row, c2, XIN, xin + c2);
+    }
+    for (int l = 0; l < 3 && ok; ++l) {
+      ok = run_layer_half(bar, tmem, l == 0 ? xs : hs, l == 0 ? S.w1 : (l == 1 ? S.w2 : S.w3), l == 0 ? XIN : HID,
+                          HID, phase, bar_id, issuer);
+      if (!ok) break;
+#pragma unroll 1
+      for (int cb = 0; cb < INF_GROUP_COLS / 16; ++cb) {
+        const int c0 = INF_GROUP_COLS * group + 16 * cb;
+        float v[16];
+        tmem_ld16(lane_addr + (uint32_t)c0, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = gelu(v[j] + S.bias[l * HID + c0 + j]);
+        put8(hs, row, c0, HID, v);
+        put8(hs, row, c0 + 8, HID, v + 8);
+      }
+    }
+    if (!ok) break;
+    ok = run_layer_half(bar, tmem, hs, S.w4, HID, YOUT, phase, bar_id, issuer);
+    if (!ok) break;
+    if (group == 0) {
+      float v[16];
+      tmem_ld16(lane_addr, v);
+      if (valid) {
+        float s[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s[k] = v[k] + S.bias[3 * HID + k];
+        if (has_skip) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) acc += S.skip[6 * k + j] * (e[j] - z[j]);
+            s[k] += acc;
+          }
+        }
+        if (w.stress)
+#pragma unroll
+          for (int k = 0; k < 6; ++k) w.stress[(size_t)p * 6 + k] = s[k];
+        float* zn = w.z + (size_t)B * 6 + (size_t)p * 6;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) zn[k] = z[k] + c * (v[6 + k] + S.bias[3 * HID + 6 + k]);
+      }
+    }
+  }
+  if (!ok && issuer && w.err) atomicExch(w.err, 1u);
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    tmem_dealloc(S.tmem, 2 * TMEM_COLS);
+  }
+}
+
 // The dynamic shared-memory limit is raised once per device and kernel (so that launches
 // recorded into a CUDA graph make no attribute call).
 int validate_common(const cib_rno_window* w) {
@@ -439,11 +603,22 @@ extern "C" int cib_rno_window_forward(const cib_rno_window* w, void* stream) {
     if (w->Z[l] && !aligned16(w->Z[l])) return CIB_EINVAL;
   if (w->gS && !w->target) return CIB_EINVAL;
   if (w->B == 0) return CIB_OK;
+  const int64_t ntiles = (w->B + TILE - 1) / TILE;
+  bool saves = w->target || w->gS || w->loss_part || w->Xt;
+  for (int l = 0; l < 3; ++l) saves = saves || w->Z[l] || w->Ht[l];
+  if (w->T == 1 && !saves && ntiles >= 2 * (int64_t)sm_count()) {
+    // inference over at least two tiles per SM: two tiles in flight per CTA
+    const size_t ibytes = sizeof(InfSmem);
+    if (allow_dynamic_smem(reinterpret_cast<const void*>(rno_infer_kernel), (int)ibytes) != CIB_OK) return CIB_ECUDA;
+    const unsigned igrid = (unsigned)std::min<int64_t>((ntiles + 1) / 2, sm_count());
+    rno_infer_kernel<<<igrid, RW_THREADS, ibytes, reinterpret_cast<cudaStream_t>(stream)>>>(*w);
+    return check_launch();
+  }
   const size_t bytes = sizeof(FwdSmem);
   if (allow_dynamic_smem(reinterpret_cast<const void*>(rno_window_forward_kernel), (int)bytes) != CIB_OK)
     return CIB_ECUDA;
   // one CTA per SM (the staged weights fill most of its shared memory), each looping over tiles
-  const unsigned grid = (unsigned)std::min<int64_t>((w->B + TILE - 1) / TILE, sm_count());
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, sm_count());
   rno_window_forward_kernel<<<grid, RW_THREADS, bytes, reinterpret_cast<cudaStream_t>(stream)>>>(*w);
   return check_launch();
 }

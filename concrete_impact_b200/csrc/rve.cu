@@ -39,37 +39,32 @@ namespace {
 
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
-// Reference-element gradient dN_a/dxi_d at Gauss point q (before the 2/h scaling).
-__device__ __forceinline__ void ref_grad(int q, int a, double g[3]) {
-  const double gp = 0.57735026918962576451;  // 1/sqrt(3)
-  const double xi = (q & 4) ? gp : -gp;
-  const double eta = (q & 2) ? gp : -gp;
-  const double zeta = (q & 1) ? gp : -gp;
-  const double sx = (a & 1) ? 1.0 : -1.0, sy = (a & 2) ? 1.0 : -1.0, sz = (a & 4) ? 1.0 : -1.0;
-  const double fx = 1.0 + sx * xi, fy = 1.0 + sy * eta, fz = 1.0 + sz * zeta;
-  g[0] = 0.125 * sx * fy * fz;
-  g[1] = 0.125 * sy * fx * fz;
-  g[2] = 0.125 * sz * fx * fy;
-}
-
 template <typename T>
 struct Grad8 {
   T x[8], y[8], z[8];
 };
 
-// Physical gradients of a box element (edges hx, hy, hz): dN/dx = dN/dxi * 2 / hx.  The
-// three reciprocals are formed once (a division per entry would be 24 FP64 divisions per
-// Gauss point in every residual pass and every CG iteration).
+// Physical gradients of a box element (edges hx, hy, hz): dN/dx = dN/dxi * 2 / hx, in the
+// element precision T.  The three reciprocals are formed once (a division per entry would
+// be 24 divisions per Gauss point in every residual pass); the node factors 1 -/+ xi are
+// selected at compile time per node.  Node a sits at (+/-1, +/-1, +/-1) by its bits 0, 1,
+// 2 and point q at (+/-, +/-, +/-) 1/sqrt(3) by its bits 2, 1, 0; dN_a/dxi = s_a / 8 (1 + s_b
+// eta)(1 + s_c zeta).
 template <typename T>
 __device__ __forceinline__ void physical_grads(int q, const RveDesc& d, Grad8<T>& G) {
-  const double sx = 2.0 / d.hx, sy = 2.0 / d.hy, sz = 2.0 / d.hz;
+  const T sx = (T)2 / (T)d.hx, sy = (T)2 / (T)d.hy, sz = (T)2 / (T)d.hz;
+  const T gp = (T)0.57735026918962576451;  // 1/sqrt(3)
+  const T xi = (q & 4) ? gp : -gp;
+  const T eta = (q & 2) ? gp : -gp;
+  const T zeta = (q & 1) ? gp : -gp;
+  const T fx[2] = {(T)1 - xi, (T)1 + xi}, fy[2] = {(T)1 - eta, (T)1 + eta}, fz[2] = {(T)1 - zeta, (T)1 + zeta};
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
-    double g[3];
-    ref_grad(q, a, g);
-    G.x[a] = (T)(g[0] * sx);
-    G.y[a] = (T)(g[1] * sy);
-    G.z[a] = (T)(g[2] * sz);
+    const int ax = a & 1, ay = (a >> 1) & 1, az = (a >> 2) & 1;
+    const T e8x = ax ? (T)0.125 : (T)-0.125, e8y = ay ? (T)0.125 : (T)-0.125, e8z = az ? (T)0.125 : (T)-0.125;
+    G.x[a] = e8x * fy[ay] * fz[az] * sx;
+    G.y[a] = e8y * fx[ax] * fz[az] * sy;
+    G.z[a] = e8z * fx[ax] * fy[ay] * sz;
   }
 }
 
@@ -144,26 +139,22 @@ struct TangentParams {
   int elastic;  // 1: use the elasticity matrix of the phase
 };
 
+// One formula for both kinds of point, so that a warp holding elastic and viscoplastic
+// points runs it once: the isotropic elasticity is K 1(x)1 + 2G P, i.e. f = 2G, c = 0.
 template <typename T>
 __device__ __forceinline__ void tangent_apply(const PhaseMat<T>& m, const TangentParams<T>& tp, const T e[6],
                                               T s[6]) {
-  if (tp.elastic) {
-    s[0] = m.C11 * e[0] + m.C12 * e[1] + m.C12 * e[2];
-    s[1] = m.C12 * e[0] + m.C11 * e[1] + m.C12 * e[2];
-    s[2] = m.C12 * e[0] + m.C12 * e[1] + m.C11 * e[2];
-    s[3] = m.G * e[3];
-    s[4] = m.G * e[4];
-    s[5] = m.G * e[5];
-    return;
-  }
+  const T f = tp.elastic ? (T)2 * m.G : tp.f;
+  const T c = tp.elastic ? (T)0 : tp.c;
   const T tr = e[0] + e[1] + e[2];
   const T ne = tp.n[0] * e[0] + tp.n[1] * e[1] + tp.n[2] * e[2] + tp.n[3] * e[3] + tp.n[4] * e[4] + tp.n[5] * e[5];
-  const T vol = m.K * tr;
-  const T third = tr * (T)(1.0 / 3.0);
+  const T cne = c * ne;
+  const T vol = m.K * tr - f * tr * (T)(1.0 / 3.0);
 #pragma unroll
-  for (int i = 0; i < 3; ++i) s[i] = vol + tp.f * (e[i] - third) + tp.c * tp.n[i] * ne;
+  for (int i = 0; i < 3; ++i) s[i] = vol + f * e[i] + cne * tp.n[i];
+  const T hf = (T)0.5 * f;
 #pragma unroll
-  for (int i = 3; i < 6; ++i) s[i] = (T)0.5 * tp.f * e[i] + tp.c * tp.n[i] * ne;
+  for (int i = 3; i < 6; ++i) s[i] = hf * e[i] + cne * tp.n[i];
 }
 
 // Butterfly reduce-scatter of 24 values over the 8 lanes of an element group: on return,
@@ -402,24 +393,27 @@ __global__ void __launch_bounds__(RVE_THREADS, sizeof(T) == 4 ? 3 : 1) rve_resid
     // its two engineering shears, so with C = K 1(x)1 + f P + c n(x)n
     //   e^T C e = K g^2 + f (2/3 g^2 + 1/2 (s1^2 + s2^2)) + c (n . e)^2
     // (elastic: C11 g^2 + G (s1^2 + s2^2)).
+    // Per point the diagonal is  A g^2 + B (s1^2 + s2^2) + c (n . e)^2  with (A, B) =
+    // (K + 2/3 f, f / 2), or (C11, G) for an elastic point (n = 0, c = 0 there); the
+    // integration weight is folded into the three coefficients.
     T f[8][3];
     bt_stress(Gr, sig, jw, f);
+    const T jwl = live ? jw : (T)0;
+    const T ca = jwl * (tp.elastic ? m.C11 : m.K + (T)(2.0 / 3.0) * tp.f);
+    const T cb = jwl * (tp.elastic ? m.G : (T)0.5 * tp.f);
+    const T cc = jwl * tp.c;
     T diag[8][3];
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       const T gx = Gr.x[b], gy = Gr.y[b], gz = Gr.z[b];
-      // (normal gradient, shear partners, n . e) for directions x, y, z (Voigt xx yy zz yz xz xy)
-      const T gn[3] = {gx, gy, gz};
-      const T sa[3] = {gz, gz, gy}, sb[3] = {gy, gx, gx};
-      const T ne[3] = {tp.n[0] * gx + tp.n[4] * gz + tp.n[5] * gy, tp.n[1] * gy + tp.n[3] * gz + tp.n[5] * gx,
-                       tp.n[2] * gz + tp.n[3] * gy + tp.n[4] * gx};
-#pragma unroll
-      for (int dd = 0; dd < 3; ++dd) {
-        const T g2 = gn[dd] * gn[dd], s2 = sa[dd] * sa[dd] + sb[dd] * sb[dd];
-        const T v = tp.elastic ? m.C11 * g2 + m.G * s2
-                               : m.K * g2 + tp.f * ((T)(2.0 / 3.0) * g2 + (T)0.5 * s2) + tp.c * ne[dd] * ne[dd];
-        diag[b][dd] = live ? jw * v : (T)0;
-      }
+      const T gx2 = gx * gx, gy2 = gy * gy, gz2 = gz * gz;
+      // n . e for the B columns of directions x, y, z (Voigt xx yy zz yz xz xy)
+      const T nx = tp.n[0] * gx + tp.n[4] * gz + tp.n[5] * gy;
+      const T ny = tp.n[1] * gy + tp.n[3] * gz + tp.n[5] * gx;
+      const T nz = tp.n[2] * gz + tp.n[3] * gy + tp.n[4] * gx;
+      diag[b][0] = ca * gx2 + cb * (gy2 + gz2) + cc * nx * nx;
+      diag[b][1] = ca * gy2 + cb * (gx2 + gz2) + cc * ny * ny;
+      diag[b][2] = ca * gz2 + cb * (gx2 + gy2) + cc * nz * nz;
     }
     T fo[3], dgo[3];
     reduce_scatter8(f, q, fo);
@@ -592,6 +586,8 @@ __device__ __forceinline__ void apply_item(const RvePcgArgs<T>& a, const ApplyIt
   tp.elastic = 1;
   tp.f = (T)0;
   tp.c = (T)0;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) tp.n[c] = (T)0;
   if (x.live && x.flag) {
     tp.elastic = 0;
 #pragma unroll
@@ -1060,6 +1056,8 @@ __global__ void __launch_bounds__(RVE_THREADS) rve_tangent_rhs_kernel(const RveT
     tp.elastic = 1;
     tp.f = (T)0;
     tp.c = (T)0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tp.n[c] = (T)0;
     if (live && a.tflag[g]) {
       tp.elastic = 0;
 #pragma unroll

@@ -134,8 +134,9 @@ def test_fused_predict_and_rollout_match_unfused() -> None:
 
 def test_persistent_forward_runs_more_tiles_than_ctas() -> None:
     """The forward window kernel runs one CTA per SM over 128-path tiles: a ragged batch of
-    313 tiles (more than one per CTA) gives the per-step GEMM path's stresses, latents and
-    per-tile window loss."""
+    313 tiles (more than one per CTA) gives the per-step GEMM path's latents and per-tile
+    window loss, and the inference kernel (two tiles in flight per CTA) its stresses and
+    latents."""
     T, B = 2, 40_000
     fused, plain = RNOSurrogate(RNOConfig(seed=8)), RNOSurrogate(RNOConfig(seed=8))
     plain.fused = False
@@ -147,10 +148,17 @@ def test_persistent_forward_runs_more_tiles_than_ctas() -> None:
     assert int(fused.err.item()) == 0 and int(plain.err.item()) == 0
     assert fused.window_loss() == pytest.approx(plain.window_loss(), rel=1e-5)
     assert _rel(fused._window["z"].cpu(), plain._window["z"].cpu()) < 1e-5
-    strain, rate, _, coef, z0 = window
+    # an inference step over more than two tiles per SM runs the two-tiles-per-CTA kernel
+    strain, rate, target, coef, z0 = window
     sf, zf, _ = fused.predict(strain[0], rate[0], z0, coef[0])
     sp, zp, _ = plain.predict(strain[0], rate[0], z0, coef[0])
     assert _rel(sf.cpu(), sp.cpu()) < 1e-5 and _rel(zf.cpu(), zp.cpu()) < 1e-5
+    # ... with the arithmetic of the training forward kernel: the same latent bit for bit
+    fused.load_window(strain[:1], rate[:1], target[:1], coef[:1], z0)
+    fused.window_step(1, B, train=False)
+    torch.cuda.synchronize()
+    assert int(fused.err.item()) == 0
+    assert torch.equal(fused._window["z"][1], zf)
 
 
 def test_training_divergence_guard_restores_finite_weights() -> None:
