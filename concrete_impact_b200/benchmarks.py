@@ -710,3 +710,46 @@ def energy_rno_workload(state_dict: dict, config, points: int = 131072, steps: i
     return {"ms": ms, "steps": steps, "points": points, "launches": _native.LAUNCHED[0] - calls0,
             "flop_per_point": energy_rno_flop(config.hidden_size, config.hidden_layers, config.latent_dimension),
             "latent_abs_max": float(box["z"].abs().max())}  # fmt: skip
+
+
+def gemm_weight_gradient_workload(rows: int = 25600, splits: int = 50, steps: int = 20, warmup: int = 3) -> dict:
+    """The training window's weight-gradient product on its own: dW (128 x 128) = dZ^T H over
+    ``rows`` = T B rows (TBPTT 50 x batch 512), split-K over ``splits`` CTAs (the split the
+    surrogate uses), fp32 partials; CUDA-event timed per launch."""
+    from . import mlp
+
+    g = torch.Generator(device="cuda").manual_seed(3)
+    a = torch.randn((128, rows), generator=g, device="cuda").to(torch.bfloat16)
+    b = torch.randn((128, rows), generator=g, device="cuda").to(torch.bfloat16)
+    part = torch.empty((splits * 128, 128), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for _ in range(warmup):
+        mlp.gemm(mlp.EPI_PARTIAL, a, b, c=part, splits=splits, err=err)
+    ms = _elapsed_ms(lambda: [mlp.gemm(mlp.EPI_PARTIAL, a, b, c=part, splits=splits, err=err) for _ in range(steps)])
+    if int(err.item()) != 0:
+        raise RuntimeError("a tensor-core wait timed out in the GEMM")
+    flop = 2.0 * 128 * 128 * rows
+    return {"ms_per_launch": ms / steps, "rows": rows, "splits": splits, "tflops": flop / (ms / steps * 1e-3) / 1e12}
+
+
+def _main(argv: list[str] | None = None) -> None:
+    """``python -m concrete_impact_b200.benchmarks rno_inference|gemm_wgrad [steps]``: time one
+    surrogate kernel on its own and print a JSON line (randomly initialised weights: the
+    kernels and their work are those of a trained surrogate)."""
+    import json
+    import sys
+
+    args = sys.argv[1:] if argv is None else argv
+    steps = int(args[1]) if len(args) > 1 else 50
+    if args and args[0] == "rno_inference":
+        from .rno import RNOConfig, RNOSurrogate
+
+        print(json.dumps(rno_inference_workload(RNOSurrogate(RNOConfig(seed=1)), steps=steps)))
+    elif args and args[0] == "gemm_wgrad":
+        print(json.dumps(gemm_weight_gradient_workload(steps=steps)))
+    else:
+        raise SystemExit("usage: python -m concrete_impact_b200.benchmarks rno_inference|gemm_wgrad [steps]")
+
+
+if __name__ == "__main__":
+    _main()
