@@ -50,6 +50,7 @@ struct GemmArgs {
   int ldht;
   int row_offset;      // row index of this GEMM's row 0 inside the transposed buffer
   unsigned int* err;   // set to 1 when a wait times out
+  int vec4;            // fp32 outputs: C 16-byte aligned and ldc a multiple of 4
 };
 
 using namespace umma;
@@ -180,7 +181,24 @@ __global__ void __launch_bounds__(GEMM_THREADS) umma_gemm_kernel(const GemmArgs 
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       }
-      if (m < a.M) {
+      const bool f32_out = EPI == EPI_F32 || EPI == EPI_BIAS_F32 || EPI == EPI_PARTIAL;
+      if (f32_out && a.vec4 && m < a.M) {
+        // fp32 rows as four 16-byte stores per 16 columns
+        float* dst = a.C + ((EPI == EPI_PARTIAL ? (size_t)blockIdx.y * a.M : 0) + m) * a.ldc + cb * 16;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float4 v = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]), __uint_as_float(r[4 * q + 2]),
+                                 __uint_as_float(r[4 * q + 3]));
+          if (EPI == EPI_BIAS_F32) {
+            const int n = cb * 16 + 4 * q;
+            v.x += a.bias[n];
+            v.y += a.bias[n + 1];
+            v.z += a.bias[n + 2];
+            v.w += a.bias[n + 3];
+          }
+          reinterpret_cast<float4*>(dst)[q] = v;
+        }
+      } else if (m < a.M) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int n = cb * 16 + j;
@@ -262,6 +280,7 @@ extern "C" int cib_mlp_gemm(int32_t epilogue, int32_t M, int32_t N, int32_t K, c
   a.ldht = ldht;
   a.row_offset = row_offset;
   a.err = err;
+  a.vec4 = (C != nullptr && aligned16(C) && (ldc % 4) == 0) ? 1 : 0;
   switch (epilogue) {
     case EPI_F32:
     case EPI_BIAS_F32:
