@@ -1,5 +1,5 @@
-"""CPU tests of host-side helpers: the PCG cluster-size heuristic, the FP32 Newton settings
-and the host training-loop baseline."""
+"""CPU tests of host-side helpers: the PCG cluster-size heuristic, the FP32 Newton settings,
+the host training-loop baseline and the kernel-timer command line."""
 
 from __future__ import annotations
 
@@ -45,3 +45,15 @@ def test_host_training_loop_learns_a_linear_map() -> None:
     out = train_windows(strain, rate, stress, coef, windows=30, batch=64, tbptt=50, lr=3e-3, threads=2)
     assert out["path_steps"] == 30 * 64 * 50 and out["seconds"] > 0
     assert out["loss_last"] < 0.2 * out["loss_first"]
+
+
+def test_kernel_timer_cli_names_its_workloads() -> None:
+    """``python -m concrete_impact_b200.benchmarks`` refuses an unknown workload with its usage
+    line (the timed workloads themselves need a GPU)."""
+    import pytest
+
+    from concrete_impact_b200.benchmarks import _main
+
+    with pytest.raises(SystemExit) as info:
+        _main(["unknown"])
+    assert "rno_inference|gemm_wgrad" in str(info.value)
