@@ -153,3 +153,32 @@ def test_sizes_beyond_32_bit_indexing_are_refused_without_a_launch() -> None:
     assert lib.cib_adam_step(65536, 65536, fake, fake, fake, fake, 1e-3, 0.9, 0.999, 1e-8, fake, None, 0, None, 0,
                              None) == -3  # fmt: skip
     assert lib.cib_splitk_reduce(65536, 65536, 1, fake, 65536, fake, 65536, None) == -3
+
+
+def test_tensor_core_entry_points_check_their_contracts_before_the_gpu() -> None:
+    """The tcgen05 GEMM and the fused surrogate window reject shapes outside their tile
+    contract (N a multiple of 16 up to 128, K a multiple of 16, 16-byte aligned rows, width
+    128) with CIB_EINVAL, and treat an empty batch as a no-op, all before any CUDA call."""
+    lib = _native.load_library()
+    fake = 256  # 16-byte aligned, never dereferenced
+    gemm = lib.cib_mlp_gemm
+    # epilogue, M, N, K, A, lda, B, ldb, splits, bias, C, ldc, Z, ldz, H, ldh, Ht, ldht, row_offset, err, stream
+    ok = dict(M=128, N=128, K=64, lda=64, ldb=64)
+
+    def call(**kw):
+        a = {**ok, **kw}
+        return gemm(0, a["M"], a["N"], a["K"], fake, a["lda"], fake, a["ldb"], 1, None, fake, a["N"], None, 0, None, 0,
+                    None, 0, 0, fake, None)  # fmt: skip
+
+    assert call(N=24) == -1 and call(N=144) == -1 and call(K=8) == -1 and call(lda=60) == -1 and call(ldb=72 + 4) == -1
+    assert call(M=0) == 0  # empty: no launch
+    w = _native.RNOWindowC()
+    w.B, w.T, w.hidden = 0, 1, 128
+    w.strain = w.rate = w.coef = w.z = w.err = fake
+    for i in range(4):
+        w.W[i], w.bias[i] = fake, fake
+    assert lib.cib_rno_window_forward(ctypes.byref(w), None) == 0  # empty batch
+    w.hidden = 96
+    assert lib.cib_rno_window_forward(ctypes.byref(w), None) == -1  # the fused kernels are width 128
+    w.hidden, w.B, w.gS = 128, 4, fake
+    assert lib.cib_rno_window_forward(ctypes.byref(w), None) == -1  # loss gradient without a target
